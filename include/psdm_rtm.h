@@ -1,0 +1,163 @@
+/*
+ * psdm_rtm.h -- C ABI of the B200 reverse-time-migration (RTM) engine.
+ *
+ * Drop-in boundary for the RTM propagators of PSDM (ejimeneztejero/PSDM).
+ * Every entry point takes plain pointers and sizes; arrays use the
+ * reference's Fortran layout (column-major, 1-based geometry indices):
+ *   model / image (ny, nx)            -> float[nx][ny]
+ *   traces (nt, NumRec)               -> float[NumRec][nt]
+ *   snapshots Fields(ny, nx_w, nslot) -> float[nslot][nx_w][ny]
+ * The caller owns host buffers; the engine owns device memory.  Calls are
+ * synchronous (results are in the caller's buffers on return), return
+ * PSDM_OK (0) on success and a negative code on failure, never exit, and
+ * leave a message for psdm_last_error().  One engine serves one host thread
+ * at a time; separate engines are independent.
+ *
+ * There is no CPU fallback: an engine on a machine without a usable CUDA
+ * device fails at psdm_engine_create with PSDM_ERR_CUDA.
+ */
+#ifndef PSDM_RTM_H
+#define PSDM_RTM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PSDM_OK = 0,
+    PSDM_ERR_ARG = -1,   /* invalid argument or geometry outside the padded grid */
+    PSDM_ERR_CUDA = -2,  /* CUDA runtime error (no device, launch failure, ...) */
+    PSDM_ERR_NOMEM = -3, /* device allocation failed (HBM budget) */
+    PSDM_ERR_STATE = -4  /* engine misuse (null engine, ...) */
+};
+
+/* Snapshot storage precision of the engine (psdm_params.precision). */
+enum {
+    PSDM_PREC_FP32 = 0,  /* plain FP32: the reference's arithmetic, bit for bit */
+    PSDM_PREC_FP16 = 1,  /* FP16 snapshots with per-snapshot power-of-two scale */
+    PSDM_PREC_BF16 = 2   /* BF16 snapshots with per-snapshot power-of-two scale */
+};
+
+/*
+ * Values the reference solvers read from module mod_parfile
+ * (src/solver_ac_forward_ram.f90:8 `USE mod_parfile, ONLY: dPML, fs`) and
+ * the driver's strategy switch (src/calculate_PSDM_RTM.f90:395,411,435).
+ */
+typedef struct psdm_params {
+    int32_t dPML;       /* C-PML thickness in cells (parfile `dPML`, default 20) */
+    int32_t fs;         /* 0 = absorbing top; otherwise free surface (parfile `free_surface`, default 1) */
+    int32_t strategy;   /* 1 = RAM solvers' statement order, 2 = disk solvers' order (strategy_num) */
+    int32_t precision;  /* PSDM_PREC_*; the *_ram drop-in entry points require PSDM_PREC_FP32 */
+} psdm_params;
+
+typedef struct psdm_engine psdm_engine;
+
+/* Last error message of the calling thread ("" if none). */
+const char* psdm_last_error(void);
+
+/* Create an engine bound to CUDA device `device`. */
+int psdm_engine_create(int32_t device, psdm_engine** out);
+int psdm_engine_destroy(psdm_engine* e);
+/* Device bytes currently held by the engine's buffer cache. */
+int64_t psdm_engine_device_bytes(const psdm_engine* e);
+/* Release the engine's cached device buffers. */
+int psdm_engine_trim(psdm_engine* e);
+
+/*
+ * Replaces dynamic_window_solver_forward_ram (src/dynamic_window.f90:54-96),
+ * which calls solver_ac_forward_ram (src/solver_ac_forward_ram.f90:4-637).
+ * Geometry in model coordinates; the window is recomputed from dd_space as
+ * the reference does.  Writes Fields(ny, nx_w, nt_snap) (slots
+ * 1..(nt-1)/store_snap; other slots untouched) and Data_synth(nt, NumRec).
+ * Fields or Data_synth may be NULL to skip that output.
+ */
+int psdm_dynamic_window_solver_forward_ram(
+    psdm_engine* e, const psdm_params* prm, int32_t NumRec,
+    const int32_t* nxSou, const int32_t* nySou, const int32_t* nxRec, const int32_t* nyRec,
+    const float* Data_source /* nt */, float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w,
+    const float* Vp_w /* (ny, nx_w) */, float dd_space, int32_t store_snap, int32_t nt_snap,
+    int32_t nt, float* Fields /* (ny, nx_w, nt_snap) or NULL */,
+    float* Data_synth /* (nt, NumRec) or NULL */);
+
+/*
+ * Replaces dynamic_window_solver_backward_ram (src/dynamic_window.f90:143-183),
+ * which calls solver_ac_backward_ram (src/solver_ac_backward_ram.f90:4-598).
+ * AdjSource(nt, NumRec) is injected at the receivers; the imaging condition
+ * is accumulated into PSDM_thread(ny, nx_w) (read, then updated in place).
+ */
+int psdm_dynamic_window_solver_backward_ram(
+    psdm_engine* e, const psdm_params* prm, int32_t NumRec,
+    const int32_t* nxSou, const int32_t* nySou, const int32_t* nxRec, const int32_t* nyRec,
+    const float* AdjSource /* (nt, NumRec) */, float dd, float dt, int32_t ny, int32_t nx,
+    int32_t nx_w, const float* Vp_w /* (ny, nx_w) */, float dd_space, int32_t store_snap,
+    int32_t nt_snap, int32_t nt, const float* Fields /* (ny, nx_w, nt_snap) */,
+    float* PSDM_thread /* (ny, nx_w), in/out */);
+
+/*
+ * One shot of RTM: replaces the per-shot block of calculate_PSDM_RTM
+ * (src/calculate_PSDM_RTM.f90:395-466) -- forward propagation, the optional
+ * half-cosine taper of the snapshot series (taper_pad_trace,
+ * src/filters.f90:20-48), time reversal of the conditioned data, backward
+ * propagation with the imaging condition.  The snapshots stay in device
+ * memory.  prm->strategy selects the RAM (1) or disk (2) solvers' statement
+ * order; prm->precision selects FP32 snapshots (bit-exact drop-in) or the
+ * mixed-precision form.  PSDM_w(ny, nx_w) is overwritten.
+ */
+int psdm_rtm_shot(
+    psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+    const int32_t* nxRec, const int32_t* nyRec, const float* Data_source /* nt_prop2 */,
+    const float* Data_target /* (nt_taper, NumRec), conditioned, not reversed */,
+    float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w /* (ny, nx_w) */,
+    float added_space, int32_t store_snap, int32_t nt_snap, int32_t nt_prop2, int32_t nt_taper,
+    int32_t taper_option, int32_t N_taper, int32_t N_zeros, float* PSDM_w /* (ny, nx_w) out */);
+
+/*
+ * Forward modelling only (the receiver output Rec_point of
+ * solver_ac_forward_ram, src/solver_ac_forward_ram.f90:567-577) without
+ * storing snapshots: synthetic shot gathers for least-squares or QC.
+ */
+int psdm_model_shot(
+    psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+    const int32_t* nxRec, const int32_t* nyRec, const float* Data_source /* nt */, float dd,
+    float dt, int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w, float dd_space,
+    int32_t nt, float* Data_synth /* (nt, NumRec) out */);
+
+/* ---- host helpers: the reference's set-up arithmetic, same FP32 order ---- */
+
+/* finite_difference_coef (src/solver_FD_coeffs.f90:1-73); coef[acc+1]. */
+void psdm_fd_coef(int32_t num, int32_t accuracy, float* coef);
+
+/*
+ * PML_coeffs (src/solver_PML_coeffs.f90:1-75): factorA/B[dn] with dn =
+ * dPML + 2*acc (zero for the first acc cells), and the corner matrices
+ * ld, rd, lu, ru (A then B) as 8 consecutive (dn, dn) column-major blocks.
+ */
+void psdm_pml_coeffs(int32_t acc, int32_t dPML, float dt, float d, int32_t dn, float* factorA,
+                     float* factorB, float* corners /* 8*dn*dn or NULL */);
+
+/* Ricker_mcs (src/get_mcs_data.f90:318-351). */
+void psdm_ricker_mcs(int32_t nt, float dt, float f0, float t0, float* S0);
+
+/* dynamic_window (src/dynamic_window.f90:1-52) for one shot. */
+void psdm_dynamic_window(int32_t NumRec, int32_t nxSou, const int32_t* nxRec, float dd, int32_t nx,
+                         float dd_space, int32_t* nx_w, int32_t* x_i, int32_t* x_f);
+
+/* taper_pad_trace (src/filters.f90:20-48), in place on trace[nt_new]. */
+void psdm_taper_pad_trace(float* trace, int32_t nt_prop, int32_t N_taper, int32_t N_zeros,
+                          int32_t nt_new);
+
+/* optimization's time step (src/optimization.f90:24-32): dt_prop, nt_prop, nt_snap. */
+void psdm_optimization_dt(float dmodel_prop, float vmax, float tfin, int32_t store_snap,
+                          float* dt_prop, int32_t* nt_prop, int32_t* nt_snap);
+
+/* normalize_psdm (src/auxiliar_PSDM.f90:1-20): PSDM = sum/fold where fold > 0. */
+void psdm_normalize_psdm(int32_t nx, int32_t ny, const float* PSDM_sum, const float* Cov_sum,
+                         float* PSDM);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSDM_RTM_H */

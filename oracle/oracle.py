@@ -1,0 +1,183 @@
+"""ctypes wrapper of the CPU oracle (liboracle_rtm.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, and only as the checker.  The CUDA engine in
+psdm_b200/ never imports this module.
+
+The oracle restates the reference's Fortran RTM solvers step by step (see the
+header of rtm_oracle.cpp for the file:line list).  Parity with the reference's
+own outputs is UNPINNED (no Fortran compiler exists here and the reference
+ships no tests or data); known-answer tests in tests/test_oracle_*.py pin it.
+
+Arrays follow the reference's Fortran layout: a model or image (ny, nx) is a
+numpy array of shape (nx, ny) in C order (column-major (ny, nx)), traces
+(nt, NumRec) are shape (NumRec, nt), Fields (ny, nx, nt_snap) is shape
+(nt_snap, nx, ny).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_rtm.so")
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_I, _F, _D = C.c_int, C.c_float, C.c_double
+
+
+def build() -> str:
+    """Compile liboracle_rtm.so with the oracle's Makefile (g++, no GPU)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_fd_coef_f.argtypes = [_I, _I, _f32p]
+        L.orc_fd_coef_d.argtypes = [_I, _I, _f64p]
+        L.orc_pml_coeffs_f.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _f32p]
+        L.orc_pml_coeffs_d.argtypes = [_I, _I, _D, _D, _I, _f64p, _f64p, _f64p]
+        L.orc_ricker_mcs.argtypes = [_I, _F, _F, _F, _f32p]
+        L.orc_taper_pad_trace_f.argtypes = [_f32p, _I, _I, _I, _I]
+        L.orc_dynamic_window.argtypes = [_I, _I, _i32p, _F, _I, _F, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
+        L.orc_solver_f.argtypes = [_I, _I, _I, _I, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _F, _F, _I, _I,
+                                   _f32p, _I, _I, _I, _f32p, _f32p]
+        L.orc_solver_dump_f.argtypes = [_I, _I, _I, _I, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _F, _F, _I, _I,
+                                        _f32p, _I, _I, _I, _f32p, _f32p, _f32p]
+        L.orc_solver_d.argtypes = [_I, _I, _I, _I, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _I, _F, _F, _I, _I,
+                                   _f32p, _I, _I, _I, _f64p, _f64p]
+        shot_args = [_I, _I, _I, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F,
+                     _I, _I, _I, _I, _I, _I, _I]
+        L.orc_rtm_shot_f.argtypes = shot_args + [_f32p, C.c_void_p]
+        L.orc_rtm_shot_d.argtypes = shot_args + [_f64p, C.c_void_p]
+        L.orc_normalize_psdm.argtypes = [_I, _I, _f32p, _f32p, _f32p]
+        _lib = L
+    return _lib
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(-1))
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def fd_coef(num: int, acc: int = 3, dtype=np.float32) -> np.ndarray:
+    c = np.zeros(acc + 1, dtype=dtype)
+    (lib().orc_fd_coef_f if dtype == np.float32 else lib().orc_fd_coef_d)(num, acc, c)
+    return c
+
+
+def pml_coeffs(dPML: int, dt: float, d: float, acc: int = 3, dtype=np.float32):
+    """factorA, factorB (dn,) and the corner matrices ld, rd, lu, ru (A then B),
+    each shape (dn, dn) indexed [col-1, row-1] (column-major)."""
+    dn = dPML + 2 * acc
+    fA = np.zeros(dn, dtype=dtype)
+    fB = np.zeros(dn, dtype=dtype)
+    corners = np.zeros(8 * dn * dn, dtype=dtype)
+    if dtype == np.float32:
+        lib().orc_pml_coeffs_f(acc, dPML, dt, d, dn, fA, fB, corners)
+    else:
+        lib().orc_pml_coeffs_d(acc, dPML, dt, d, dn, fA, fB, corners)
+    c = corners.reshape(8, dn, dn)
+    names = ["ldA", "rdA", "luA", "ruA", "ldB", "rdB", "luB", "ruB"]
+    return fA, fB, {n: c[q] for q, n in enumerate(names)}
+
+
+def ricker_mcs(nt: int, dt: float, f0: float, t0: float = 0.0) -> np.ndarray:
+    s = np.zeros(nt, dtype=np.float32)
+    lib().orc_ricker_mcs(nt, dt, f0, t0, s)
+    return s
+
+
+def taper_pad_trace(trace, nt_prop: int, N_taper: int, N_zeros: int) -> np.ndarray:
+    t = _f32(trace).copy()
+    lib().orc_taper_pad_trace_f(t, nt_prop, N_taper, N_zeros, t.size)
+    return t
+
+
+def dynamic_window(nxSou: int, nxRec, dd: float, nx: int, dd_space: float):
+    r = _i32(nxRec)
+    a, b, c = _I(), _I(), _I()
+    lib().orc_dynamic_window(r.size, int(nxSou), r, dd, nx, dd_space, C.byref(a), C.byref(b), C.byref(c))
+    return a.value, b.value, c.value  # nx_w, x_i, x_f
+
+
+def solver(iprop: int, *, dPML: int, fs: int, nxSou, nySou, nxRec, nyRec, S, dmodel: float, dt: float,
+           vp, store_snap: int, nt_snap: int, nt: int, Fields=None, disk_mode: int = 0,
+           dtype=np.float32):
+    """One propagator call in window coordinates (solver_ac_forward_ram /
+    solver_ac_backward_ram).  vp: (nx, ny) float32.  Forward (iprop=1)
+    returns (Fields, Rec); backward (iprop=2) returns the image (nx, ny)."""
+    vp = _f32(vp)
+    nx, ny = vp.shape
+    nrec = len(np.atleast_1d(nxRec))
+    S = _f32(S).reshape(-1)
+    if Fields is None:
+        Fields = np.zeros((nt_snap, nx, ny), dtype=dtype)
+    Fields = np.ascontiguousarray(Fields, dtype=dtype)
+    if iprop == 1:
+        out = np.zeros((nrec, nt), dtype=dtype)
+    else:
+        out = np.zeros((nx, ny), dtype=dtype)
+    args = (iprop, disk_mode, dPML, fs, nrec, _i32(nxSou), _i32(nySou), _i32(nxRec), _i32(nyRec))
+    if dtype == np.float32:
+        lib().orc_solver_f(*args, S, dmodel, dt, ny, nx, vp, store_snap, nt_snap, nt, Fields, out)
+    else:
+        lib().orc_solver_d(*args, S, S.size, dmodel, dt, ny, nx, vp, store_snap, nt_snap, nt, Fields, out)
+    return (Fields, out) if iprop == 1 else out
+
+
+def forward_dump_p(*, dPML, fs, nxSou, nySou, nxRec, nyRec, S, dmodel, dt, vp, nt, disk_mode=0):
+    """Forward propagation for nt steps; returns the padded p (nxt, nyt) after
+    the last step (debugging aid for parity failures)."""
+    vp = _f32(vp)
+    nx, ny = vp.shape
+    dn = dPML + 6
+    nrec = len(np.atleast_1d(nxRec))
+    F = np.zeros((max(nt, 1), nx, ny), dtype=np.float32)
+    out = np.zeros((nrec, nt), dtype=np.float32)
+    pd = np.zeros((nx + 2 * dn, ny + 2 * dn), dtype=np.float32)
+    lib().orc_solver_dump_f(1, disk_mode, dPML, fs, nrec, _i32(nxSou), _i32(nySou), _i32(nxRec), _i32(nyRec),
+                            _f32(S).reshape(-1), dmodel, dt, ny, nx, vp, 1, nt, nt, F, out, pd)
+    return pd
+
+
+def rtm_shot(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target,
+             dd: float, dt: float, nx: int, vp_w, added_space: float, store_snap: int, nt_snap: int,
+             nt_prop2: int, nt_taper: int, taper_option: int = 0, N_taper: int = 1, N_zeros: int = 0,
+             disk_mode: int = 0, dtype=np.float32, want_synth: bool = False):
+    """calculate_PSDM_RTM.f90:395-466 for one shot.  Returns the window image
+    (nx_w, ny) and, if asked, the forward receiver traces (NumRec, nt_prop2)."""
+    vp_w = _f32(vp_w)
+    nx_w, ny = vp_w.shape
+    nrec = len(np.atleast_1d(nxRec))
+    img = np.zeros((nx_w, ny), dtype=dtype)
+    synth = np.zeros((nrec, nt_prop2), dtype=dtype) if want_synth else None
+    fn = lib().orc_rtm_shot_f if dtype == np.float32 else lib().orc_rtm_shot_d
+    fn(disk_mode, dPML, fs, nrec, int(nxSou), int(nySou), _i32(nxRec), _i32(nyRec),
+       _f32(Data_source).reshape(-1), _f32(Data_target).reshape(-1), dd, dt, ny, nx, nx_w, vp_w,
+       added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, img,
+       synth.ctypes.data if synth is not None else None)
+    return (img, synth) if want_synth else img
+
+
+def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
+    a = _f32(psdm_sum)
+    b = _f32(cov_sum)
+    out = np.zeros_like(a)
+    nx, ny = a.shape
+    lib().orc_normalize_psdm(nx, ny, a, b, out)
+    return out

@@ -1,0 +1,88 @@
+"""ctypes binding of libpsdm_rtm.so (the C ABI declared in include/psdm_rtm.h).
+
+The library is the product: there is no CPU fallback.  Loading fails loudly
+if the shared library has not been built (python -m psdm_b200.build).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libpsdm_rtm.so")
+
+PSDM_OK, PSDM_ERR_ARG, PSDM_ERR_CUDA, PSDM_ERR_NOMEM, PSDM_ERR_STATE = 0, -1, -2, -3, -4
+PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
+
+# Every symbol include/psdm_rtm.h declares (checked by tests/test_abi.py).
+EXPORTS = [
+    "psdm_last_error", "psdm_engine_create", "psdm_engine_destroy", "psdm_engine_device_bytes",
+    "psdm_engine_trim", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
+    "psdm_rtm_shot", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
+    "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
+]
+
+
+class Params(C.Structure):
+    _fields_ = [("dPML", C.c_int32), ("fs", C.c_int32), ("strategy", C.c_int32), ("precision", C.c_int32)]
+
+
+class PsdmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"psdm error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_I, _F, _P = C.c_int32, C.c_float, C.c_void_p
+
+
+def lib():
+    """Load libpsdm_rtm.so (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m psdm_b200.build` "
+                          "(the RTM engine has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    L.psdm_last_error.restype = C.c_char_p
+    L.psdm_engine_create.argtypes = [_I, C.POINTER(_P)]
+    L.psdm_engine_destroy.argtypes = [_P]
+    L.psdm_engine_device_bytes.argtypes = [_P]
+    L.psdm_engine_device_bytes.restype = C.c_int64
+    L.psdm_engine_trim.argtypes = [_P]
+    PP = C.POINTER(Params)
+    L.psdm_dynamic_window_solver_forward_ram.argtypes = [
+        _P, PP, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _I, _I, _P, _P]
+    L.psdm_dynamic_window_solver_backward_ram.argtypes = [
+        _P, PP, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _I, _I, _P, _f32p]
+    L.psdm_rtm_shot.argtypes = [
+        _P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _I, _I, _I, _I, _I, _I,
+        _f32p]
+    L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
+    L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
+    L.psdm_fd_coef.restype = None
+    L.psdm_pml_coeffs.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _P]
+    L.psdm_pml_coeffs.restype = None
+    L.psdm_ricker_mcs.argtypes = [_I, _F, _F, _F, _f32p]
+    L.psdm_ricker_mcs.restype = None
+    L.psdm_dynamic_window.argtypes = [_I, _I, _i32p, _F, _I, _F, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]
+    L.psdm_dynamic_window.restype = None
+    L.psdm_taper_pad_trace.argtypes = [_f32p, _I, _I, _I, _I]
+    L.psdm_taper_pad_trace.restype = None
+    L.psdm_optimization_dt.argtypes = [_F, _F, _F, _I, C.POINTER(_F), C.POINTER(_I), C.POINTER(_I)]
+    L.psdm_optimization_dt.restype = None
+    L.psdm_normalize_psdm.argtypes = [_I, _I, _f32p, _f32p, _f32p]
+    L.psdm_normalize_psdm.restype = None
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != PSDM_OK:
+        raise PsdmError(rc, lib().psdm_last_error().decode(errors="replace"))

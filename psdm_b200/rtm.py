@@ -1,0 +1,196 @@
+"""Python face of the RTM engine, mirroring the reference's solver interface.
+
+Names, argument meaning and order follow the Fortran routines they replace
+(src/dynamic_window.f90:54-183, src/calculate_PSDM_RTM.f90:395-466), so
+a driver written against the reference reads the same.  Everything runs
+through the C ABI of libpsdm_rtm.so (include/psdm_rtm.h).
+
+Array layout is the reference's column-major order expressed as C-order numpy
+arrays: a model or image (ny, nx) is an array of shape (nx, ny); traces
+(nt, NumRec) are shape (NumRec, nt); Fields (ny, nx_w, nt_snap) is shape
+(nt_snap, nx_w, ny).  Geometry indices are 1-based model coordinates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(-1))
+
+
+@dataclass
+class Params:
+    """Module globals of mod_parfile read by the solvers, plus the strategy
+    switch and the engine precision (PSDM_PREC_*)."""
+    dPML: int = 20
+    fs: int = 1
+    strategy: int = 1
+    precision: int = L.PREC_FP32
+
+    def c(self) -> L.Params:
+        return L.Params(self.dPML, self.fs, self.strategy, self.precision)
+
+
+class Engine:
+    """One RTM engine bound to a CUDA device (owns device memory)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        L.check(L.lib().psdm_engine_create(device, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            L.lib().psdm_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self) -> int:
+        return int(L.lib().psdm_engine_device_bytes(self._h))
+
+    def trim(self):
+        L.check(L.lib().psdm_engine_trim(self._h))
+
+    # ---- reference-named entry points ------------------------------------
+    def dynamic_window_solver_forward_ram(self, prm: Params, nxSou, nySou, nxRec, nyRec, Data_source, dd, dt,
+                                          ny, nx, nx_w, Vp_w, dd_space, store_snap, nt_snap, nt,
+                                          Fields=None, Data_synth=None):
+        """src/dynamic_window.f90:54-96.  Fills Fields (nt_snap, nx_w, ny) and
+        Data_synth (NumRec, nt) in place if given; returns (Fields, Data_synth)."""
+        nxRec = _i32(nxRec)
+        nrec = nxRec.size
+        Vp_w = _f32(Vp_w)
+        assert Vp_w.shape == (nx_w, ny)
+        S = _f32(Data_source).reshape(-1)
+        assert S.size >= nt
+        fptr = synptr = None
+        if Fields is not None:
+            assert Fields.dtype == np.float32 and Fields.flags.c_contiguous and Fields.size >= nt_snap * nx_w * ny
+            fptr = Fields.ctypes.data
+        if Data_synth is not None:
+            assert Data_synth.dtype == np.float32 and Data_synth.flags.c_contiguous and Data_synth.size >= nrec * nt
+            synptr = Data_synth.ctypes.data
+        L.check(L.lib().psdm_dynamic_window_solver_forward_ram(
+            self._h, C.byref(prm.c()), nrec, _i32(nxSou), _i32(nySou), nxRec, _i32(nyRec), S, dd, dt, ny, nx,
+            nx_w, Vp_w, dd_space, store_snap, nt_snap, nt, fptr, synptr))
+        return Fields, Data_synth
+
+    def dynamic_window_solver_backward_ram(self, prm: Params, nxSou, nySou, nxRec, nyRec, AdjSource, dd, dt,
+                                           ny, nx, nx_w, Vp_w, dd_space, store_snap, nt_snap, nt, Fields,
+                                           PSDM_thread):
+        """src/dynamic_window.f90:143-183.  PSDM_thread (nx_w, ny) is updated in place."""
+        nxRec = _i32(nxRec)
+        adj = _f32(AdjSource)
+        assert adj.size >= nxRec.size * nt
+        assert PSDM_thread.dtype == np.float32 and PSDM_thread.flags.c_contiguous
+        F = _f32(Fields) if Fields is not None else None
+        L.check(L.lib().psdm_dynamic_window_solver_backward_ram(
+            self._h, C.byref(prm.c()), nxRec.size, _i32(nxSou), _i32(nySou), nxRec, _i32(nyRec), adj.reshape(-1),
+            dd, dt, ny, nx, nx_w, _f32(Vp_w), dd_space, store_snap, nt_snap, nt,
+            F.ctypes.data if F is not None else None, PSDM_thread))
+        return PSDM_thread
+
+    def rtm_shot(self, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target, dd, dt, ny,
+                 nx, nx_w, Vp_w, added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option=0, N_taper=1,
+                 N_zeros=0, PSDM_w=None):
+        """src/calculate_PSDM_RTM.f90:395-466 for one shot; returns PSDM_w (nx_w, ny)."""
+        nxRec = _i32(nxRec)
+        if PSDM_w is None:
+            PSDM_w = np.zeros((nx_w, ny), dtype=np.float32)
+        tgt = _f32(Data_target)
+        assert tgt.size == nxRec.size * nt_taper
+        L.check(L.lib().psdm_rtm_shot(
+            self._h, C.byref(prm.c()), nxRec.size, int(nxSou), int(nySou), nxRec, _i32(nyRec),
+            _f32(Data_source).reshape(-1), tgt.reshape(-1), dd, dt, ny, nx, nx_w, _f32(Vp_w), added_space,
+            store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, PSDM_w))
+        return PSDM_w
+
+    def model_shot(self, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, dd, dt, ny, nx, nx_w,
+                   Vp_w, dd_space, nt):
+        """Forward modelling (Rec_point of solver_ac_forward_ram); returns (NumRec, nt)."""
+        nxRec = _i32(nxRec)
+        out = np.zeros((nxRec.size, nt), dtype=np.float32)
+        L.check(L.lib().psdm_model_shot(
+            self._h, C.byref(prm.c()), nxRec.size, int(nxSou), int(nySou), nxRec, _i32(nyRec),
+            _f32(Data_source).reshape(-1), dd, dt, ny, nx, nx_w, _f32(Vp_w), dd_space, nt, out))
+        return out
+
+
+# ---- host helpers (reference set-up arithmetic, run in the library) --------
+
+def fd_coef(num: int, acc: int = 3) -> np.ndarray:
+    c = np.zeros(acc + 1, dtype=np.float32)
+    L.lib().psdm_fd_coef(num, acc, c)
+    return c
+
+
+def pml_coeffs(dPML: int, dt: float, d: float, acc: int = 3, corners: bool = False):
+    dn = dPML + 2 * acc
+    fA = np.zeros(dn, dtype=np.float32)
+    fB = np.zeros(dn, dtype=np.float32)
+    cm = np.zeros(8 * dn * dn, dtype=np.float32) if corners else None
+    L.lib().psdm_pml_coeffs(acc, dPML, dt, d, dn, fA, fB, cm.ctypes.data if cm is not None else None)
+    if not corners:
+        return fA, fB
+    c = cm.reshape(8, dn, dn)
+    names = ["ldA", "rdA", "luA", "ruA", "ldB", "rdB", "luB", "ruB"]
+    return fA, fB, {n: c[q] for q, n in enumerate(names)}
+
+
+def ricker_mcs(nt: int, dt: float, f0: float, t0: float = 0.0) -> np.ndarray:
+    s = np.zeros(nt, dtype=np.float32)
+    L.lib().psdm_ricker_mcs(nt, dt, f0, t0, s)
+    return s
+
+
+def dynamic_window(nxSou: int, nxRec, dd: float, nx: int, dd_space: float):
+    """Returns (nx_w, x_i, x_f) (src/dynamic_window.f90:1-52)."""
+    r = _i32(nxRec)
+    a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+    L.lib().psdm_dynamic_window(r.size, int(nxSou), r, dd, nx, dd_space, C.byref(a), C.byref(b), C.byref(c))
+    return a.value, b.value, c.value
+
+
+def taper_pad_trace(trace, nt_prop: int, N_taper: int, N_zeros: int) -> np.ndarray:
+    t = _f32(trace).copy()
+    L.lib().psdm_taper_pad_trace(t, nt_prop, N_taper, N_zeros, t.size)
+    return t
+
+
+def optimization_dt(dmodel_prop: float, vmax: float, tfin: float, store_snap: int = 1):
+    """Returns (dt_prop, nt_prop, nt_snap) (src/optimization.f90:24-32)."""
+    dt, ntp, nts = C.c_float(), C.c_int32(), C.c_int32()
+    L.lib().psdm_optimization_dt(dmodel_prop, vmax, tfin, store_snap, C.byref(dt), C.byref(ntp), C.byref(nts))
+    return dt.value, ntp.value, nts.value
+
+
+def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
+    a, b = _f32(psdm_sum), _f32(cov_sum)
+    out = np.zeros_like(a)
+    nx, ny = a.shape
+    L.lib().psdm_normalize_psdm(nx, ny, a, b, out)
+    return out
