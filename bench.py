@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""RTM throughput benchmark (shots/s) for the B200 engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One step = one RTM shot of the production-size drop-in configuration
+(config 2: 1200 x 4000 cells at 6.25 m, window 1200 x 1136, CPML 50, free
+surface, dt 0.5 ms, nt 8000, 480 receivers): forward propagation with all
+8000 FP32 snapshots kept in HBM (43.6 GB), backward propagation with the
+imaging condition, and the window stacked into the full image.  Inputs are
+seeded synthetic data (see psdm_b200/synth.py): smoothed migration model,
+Ricker source, observed data forward-modelled by the engine on the true model
+with the direct arrival muted.
+
+`value` is timed with CUDA events around K shots whose inputs are already in
+HBM; `e2e` times K shots through the C-ABI call psdm_rtm_shot with pinned
+host buffers (H2D of model + traces and D2H of the image inside the timed
+region).  Each shot streams 87 GB of snapshots through HBM, so every timed
+step is far larger than L2 (no explicit flush needed).
+
+Under torchrun (N > 1) every rank migrates its own shots (round-robin, as
+calculate_PSDM_RTM.f90:168) and the per-round images are summed with one
+all-reduce per round (the reference's MPI_ALLREDUCE, :493-494).
+
+--impl reference times the reference's CPU algorithm on the host cores: the
+reference is Fortran and cannot be compiled here (no Fortran compiler), so
+its step-by-step C++ restatement (oracle/) stands in, one shot per process
+as the reference runs one shot per MPI rank.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# ---- workload (config 2) --------------------------------------------------
+NY, NX, DD, DT, NT, DPML, F0 = 1200, 4000, 6.25, 5e-4, 8000, 50, 20.0
+ADDED_SPACE = 500.0
+WORKLOAD = "rtm_config2_1200x4000_dx6.25_nt8000_cpml50_480ch_fp32"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def grid_cells(ny, nx_w, dpml, fs=1):
+    dn = dpml + 6
+    nyt, nxt = ny + 2 * dn, nx_w + 2 * dn
+    rows = nyt - dn if fs else nyt
+    return dict(dn=dn, nyt=nyt, nxt=nxt, n_pad=nyt * nxt, n_act=rows * nxt, n_int=ny * nx_w,
+                n_xpml=2 * dn * rows, n_zpml=(dn if fs else 2 * dn) * nxt)
+
+
+def algorithmic_bytes(ny, nx_w, dpml, fs=1):
+    """Compulsory bytes of one fused step (per launch), plain FP32:
+    16 B per updated cell (read p, read+write p1/p3, read c2), 16 B per PML
+    cell per direction (phi in/out, chi read+write), snapshot 4 B per interior
+    cell (forward write / backward read) and the image read+write (8 B per
+    interior cell, backward)."""
+    g = grid_cells(ny, nx_w, dpml, fs)
+    base = 16 * g["n_act"] + 16 * (g["n_xpml"] + g["n_zpml"])
+    return base + 4 * g["n_int"], base + 12 * g["n_int"], g
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                smax = float(r[1])
+                for n, v in zip(names, r[4:8]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---- CPU arm (oracle restatement) -------------------------------------------
+
+def _cpu_worker(args):
+    """One process = one shot sample of the CPU restatement (C2 window, nt_s steps)."""
+    nt_s, seed = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from psdm_b200 import synth
+    sv = synth.config2_survey(4)
+    s = seed % sv.nshots
+    nx_w, x_i, x_f = O.dynamic_window(int(sv.nxSou[s]), sv.nxRec[s], DD, NX, ADDED_SPACE)
+    vp = np.full((nx_w, NY), 2000.0, dtype=np.float32)
+    src = O.ricker_mcs(nt_s, DT, F0)
+    tgt = np.random.default_rng(seed).standard_normal((sv.nrec, nt_s)).astype(np.float32)
+    t0 = time.perf_counter()
+    O.rtm_shot(dPML=DPML, fs=1, nxSou=int(sv.nxSou[s]), nySou=int(sv.nySou[s]), nxRec=sv.nxRec[s],
+               nyRec=sv.nyRec[s], Data_source=src, Data_target=tgt, dd=DD, dt=DT, nx=NX, vp_w=vp,
+               added_space=ADDED_SPACE, store_snap=1, nt_snap=nt_s, nt_prop2=nt_s, nt_taper=nt_s)
+    return time.perf_counter() - t0, nx_w
+
+
+def cpu_sample(procs: int, nt_s: int):
+    """Run `procs` shot samples in parallel; extrapolate to full shots/s."""
+    from oracle import oracle as O
+    O.build() if not os.path.exists(O._LIB_PATH) else None
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(nt_s, i) for i in range(procs)])
+    wall = time.perf_counter() - t0
+    per_sample = max(r[0] for r in res)
+    per_shot = per_sample * (2 * (NT - 1)) / (2 * (nt_s - 1))
+    return {"shots_per_s": procs / per_shot, "sec_per_shot": per_shot, "sample_s": per_sample, "wall_s": wall,
+            "nx_w": res[0][1]}
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_procs(max_procs: int) -> int:
+    n = host_cores()
+    try:
+        import psutil
+        n = min(n, max(1, int(psutil.virtual_memory().available / (1.2 * 2 ** 30))))
+    except Exception:
+        pass
+    return max(1, min(n, max_procs))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    procs = cpu_procs(64)
+    nt_s = 12
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(procs, nt_s)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["shots_per_s"] for r in vals])
+    sample = (f"{procs} processes x one config-2 shot sample each ({nt_s} forward + {nt_s} backward steps on "
+              f"the {NY}x{vals[0]['nx_w']} window), extrapolated to nt={NT}")
+    line = {"impl": "reference", "metric": "rtm_shots_per_s", "value": v, "unit": "shots/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cpu": "reference algorithm, C++ restatement (oracle/)",
+                       "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": v, "unit": "shots/s", "cores": procs, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- GPU arm -----------------------------------------------------------------
+
+def build_inputs(engine, torch, dev, shots, survey, vel_true, vel_mig, prm):
+    """Device-resident inputs of each shot (model window, source, observed data)."""
+    from psdm_b200 import rtm, synth
+    src = rtm.ricker_mcs(NT, DT, F0)
+    d_src = torch.from_numpy(src).to(dev)
+    items = []
+    for s in shots:
+        nxS, nyS = int(survey.nxSou[s]), int(survey.nySou[s])
+        nxR, nyR = survey.nxRec[s], survey.nyRec[s]
+        nx_w, x_i, x_f = rtm.dynamic_window(nxS, nxR, DD, NX, ADDED_SPACE)
+        vt = np.ascontiguousarray(vel_true[x_i - 1:x_f])
+        vm = np.ascontiguousarray(vel_mig[x_i - 1:x_f])
+        obs = engine.model_shot(prm, nxS, nyS, nxR, nyR, src, DD, DT, NY, NX, nx_w, vt, ADDED_SPACE, NT)
+        obs = synth.mute_direct(obs, survey.pos_rec[s] - survey.pos_shot[s], DT)
+        items.append(dict(nxSou=nxS, nySou=nyS, nxRec=nxR, nyRec=nyR, nx_w=nx_w, x_i=x_i, x_f=x_f,
+                          vp_h=vm, obs_h=np.ascontiguousarray(obs, dtype=np.float32),
+                          d_vp=torch.from_numpy(vm).to(dev), d_obs=torch.from_numpy(obs).to(dev)))
+    return d_src, src, items
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from psdm_b200 import rtm, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    engine = rtm.Engine(local)
+    stream = torch.cuda.current_stream(dev)
+    engine.set_stream(stream.cuda_stream)
+    prm = rtm.Params(dPML=DPML, fs=1, strategy=1)
+
+    survey = synth.config2_survey(200)
+    vel_true = synth.config2_model(seed=2)
+    vel_mig = synth.smooth_model(vel_true, 100.0, DD)
+    n_total = args.warmup + args.steps
+    # round-robin shots: icount = (itimes-1)*numtasks + rank + line_i
+    my_shots = [(i * world + rank) % survey.nshots for i in range(n_total)]
+    uniq = sorted(set(my_shots))
+    d_src, h_src, items_u = build_inputs(engine, torch, dev, uniq, survey, vel_true, vel_mig, prm)
+    by_shot = dict(zip(uniq, items_u))
+    items = [by_shot[s] for s in my_shots]
+
+    psdm_sum = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
+    cov_sum = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
+    d_img = torch.zeros((max(it["nx_w"] for it in items), NY), dtype=torch.float32, device=dev)
+    thread_img = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
+    thread_cov = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
+
+    def one_round(it):
+        nx_w = it["nx_w"]
+        engine.rtm_shot_device(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], d_src.data_ptr(),
+                               it["d_obs"].data_ptr(), DD, DT, NY, NX, nx_w, it["d_vp"].data_ptr(), ADDED_SPACE, 1,
+                               NT, NT, NT, 0, 1, 0, d_img.data_ptr())
+        thread_img.zero_()
+        thread_cov.zero_()
+        thread_img[it["x_i"] - 1:it["x_f"]] = d_img[:nx_w]
+        thread_cov[it["x_i"] - 1:it["x_f"]] = 1.0
+        if world > 1:
+            dist.all_reduce(thread_img)
+            dist.all_reduce(thread_cov)
+        psdm_sum.add_(thread_img)
+        cov_sum.add_(thread_cov)
+
+    for i in range(args.warmup):
+        one_round(items[i])
+    torch.cuda.synchronize(dev)
+    engine.reset_stats()
+    engine.set_profiling(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for i in range(args.warmup, n_total):
+            one_round(items[i])
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    st = engine.stats()
+    engine.set_profiling(False)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (per-launch time from CUDA events)
+    nx_w0 = items[args.warmup]["nx_w"]
+    fwd_b, bwd_b, g = algorithmic_bytes(NY, nx_w0, DPML, 1)
+    fwd_us = st["fwd_ms"] * 1e3 / max(st["fwd_steps"], 1)
+    bwd_us = st["bwd_ms"] * 1e3 / max(st["bwd_steps"], 1)
+    dom = "bwd" if st["bwd_ms"] >= st["fwd_ms"] else "fwd"
+    peak, peak_kind = _peaks()
+    bytes_dom = bwd_b if dom == "bwd" else fwd_b
+    us_dom = bwd_us if dom == "bwd" else fwd_us
+    achieved = bytes_dom / (us_dom * 1e-6) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("step_kernel_bwd" if dom == "bwd" else "step_kernel_fwd")
+
+    # end-to-end through the C ABI with pinned host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        pin = [(torch.from_numpy(it["vp_h"]).pin_memory(), torch.from_numpy(it["obs_h"]).pin_memory(),
+                torch.empty((it["nx_w"], NY), dtype=torch.float32).pin_memory()) for it in items[args.warmup:]]
+        h_src = torch.from_numpy(h_src).pin_memory()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for it, (vp_p, obs_p, img_p) in zip(items[args.warmup:], pin):
+            engine.rtm_shot(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], h_src.numpy(), obs_p.numpy(),
+                            DD, DT, NY, NX, it["nx_w"], vp_p.numpy(), ADDED_SPACE, 1, NT, NT, NT, 0, 1, 0,
+                            PSDM_w=img_p.numpy())
+        torch.cuda.synchronize(dev)
+        el = torch.tensor([time.perf_counter() - t0], device=dev)
+        if world > 1:
+            dist.all_reduce(el, op=dist.ReduceOp.MAX)
+        it0 = items[args.warmup]
+        h2d = 4 * (NY * it0["nx_w"] + NT + it0["obs_h"].size) + 8 * it0["obs_h"].shape[0]
+        d2h = 4 * NY * it0["nx_w"]
+        e2e = {"value": world * args.steps / float(el.item()), "unit": "shots/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "api": "psdm_rtm_shot (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_sample(cpu_procs(32), 12)
+        cpu = {"value": r["shots_per_s"], "unit": "shots/s", "cores": cpu_procs(32), "kind": "port",
+               "sample": f"{cpu_procs(32)} processes x one config-2 shot sample each (12 forward + 12 backward "
+                         f"steps of the C++ restatement), extrapolated to nt={NT}; {r['sec_per_shot']:.0f} s/shot"}
+
+    if rank == 0:
+        gcell = world * args.steps * 2 * (NT - 1) * g["n_pad"] / (ms_max / 1e3) / 1e9
+        line = {"metric": "rtm_shots_per_s", "value": value, "unit": "shots/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "engine": "plain FP32 drop-in (bit-exact)", "nx_w": nx_w0,
+                           "cells_padded": g["n_pad"], "snapshots_gb": round(4 * g["n_int"] * (NT - 1) / 1e9, 1),
+                           "l2": "inputs larger than L2 (87 GB of snapshots streamed per step)",
+                           "parallelism": f"shots x{world}"},
+                "gcell_upd_per_s": gcell,
+                "kernel": {"fwd_us_per_step": fwd_us, "bwd_us_per_step": bwd_us, "fwd_bytes": fwd_b,
+                           "bwd_bytes": bwd_b},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": f"step_kernel<{dom}>",
+                             "peak_kind": peak_kind},
+                "gpu_launches": int(st["launches"]),
+                "clocks": clk.summary(),
+                "e2e": e2e,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--nt", type=int, default=None,
+                    help="override the record length (small cases for ncu captures only; not a bench value)")
+    args = ap.parse_args()
+    if args.nt:
+        global NT, WORKLOAD
+        NT = args.nt
+        WORKLOAD = WORKLOAD.replace("nt8000", f"nt{NT}")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -64,6 +64,26 @@ int psdm_engine_destroy(psdm_engine* e);
 int64_t psdm_engine_device_bytes(const psdm_engine* e);
 /* Release the engine's cached device buffers. */
 int psdm_engine_trim(psdm_engine* e);
+/*
+ * Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*); NULL restores the engine's own stream.  No reference counterpart:
+ * lets a host framework order the engine with its own device work.
+ */
+int psdm_engine_set_stream(psdm_engine* e, void* stream);
+
+/* Counters of the engine (no reference counterpart; the reference only prints). */
+typedef struct psdm_stats {
+    int64_t launches;   /* kernels launched by the engine */
+    int64_t fwd_steps;  /* forward time steps */
+    int64_t bwd_steps;  /* backward time steps */
+    int64_t shots;      /* shots timed while profiling was on */
+    double fwd_ms;      /* device time of the forward passes of those shots */
+    double bwd_ms;      /* device time of the backward passes of those shots */
+} psdm_stats;
+/* Turn per-shot CUDA-event timing of the forward and backward passes on/off. */
+int psdm_engine_set_profiling(psdm_engine* e, int32_t on);
+int psdm_engine_stats(psdm_engine* e, psdm_stats* out);
+int psdm_engine_reset_stats(psdm_engine* e);
 
 /*
  * Replaces dynamic_window_solver_forward_ram (src/dynamic_window.f90:54-96),
@@ -112,6 +132,20 @@ int psdm_rtm_shot(
     float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w /* (ny, nx_w) */,
     float added_space, int32_t store_snap, int32_t nt_snap, int32_t nt_prop2, int32_t nt_taper,
     int32_t taper_option, int32_t N_taper, int32_t N_zeros, float* PSDM_w /* (ny, nx_w) out */);
+
+/*
+ * psdm_rtm_shot with every array already in device memory (d_* pointers are
+ * device pointers; nxRec/nyRec stay on the host).  Asynchronous: work is
+ * queued on the engine's stream and the call returns without waiting.  Same
+ * arithmetic as psdm_rtm_shot; for host frameworks that keep models, data
+ * and images resident in HBM across shots.
+ */
+int psdm_rtm_shot_device(
+    psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+    const int32_t* nxRec, const int32_t* nyRec, const float* d_Data_source,
+    const float* d_Data_target, float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w,
+    const float* d_Vp_w, float added_space, int32_t store_snap, int32_t nt_snap, int32_t nt_prop2,
+    int32_t nt_taper, int32_t taper_option, int32_t N_taper, int32_t N_zeros, float* d_PSDM_w);
 
 /*
  * Forward modelling only (the receiver output Rec_point of

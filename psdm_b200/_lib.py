@@ -18,14 +18,20 @@ PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
 # Every symbol include/psdm_rtm.h declares (checked by tests/test_abi.py).
 EXPORTS = [
     "psdm_last_error", "psdm_engine_create", "psdm_engine_destroy", "psdm_engine_device_bytes",
-    "psdm_engine_trim", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
-    "psdm_rtm_shot", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
+    "psdm_engine_trim", "psdm_engine_set_stream", "psdm_engine_set_profiling", "psdm_engine_stats",
+    "psdm_engine_reset_stats", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
+    "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
 ]
 
 
 class Params(C.Structure):
     _fields_ = [("dPML", C.c_int32), ("fs", C.c_int32), ("strategy", C.c_int32), ("precision", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("fwd_steps", C.c_int64), ("bwd_steps", C.c_int64), ("shots", C.c_int64),
+                ("fwd_ms", C.c_double), ("bwd_ms", C.c_double)]
 
 
 class PsdmError(RuntimeError):
@@ -56,6 +62,10 @@ def lib():
     L.psdm_engine_device_bytes.argtypes = [_P]
     L.psdm_engine_device_bytes.restype = C.c_int64
     L.psdm_engine_trim.argtypes = [_P]
+    L.psdm_engine_set_stream.argtypes = [_P, _P]
+    L.psdm_engine_set_profiling.argtypes = [_P, _I]
+    L.psdm_engine_stats.argtypes = [_P, C.POINTER(Stats)]
+    L.psdm_engine_reset_stats.argtypes = [_P]
     PP = C.POINTER(Params)
     L.psdm_dynamic_window_solver_forward_ram.argtypes = [
         _P, PP, _I, _i32p, _i32p, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _I, _I, _P, _P]
@@ -64,6 +74,8 @@ def lib():
     L.psdm_rtm_shot.argtypes = [
         _P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _I, _I, _I, _I, _I, _I,
         _f32p]
+    L.psdm_rtm_shot_device.argtypes = [
+        _P, PP, _I, _I, _I, _i32p, _i32p, _P, _P, _F, _F, _I, _I, _I, _P, _F, _I, _I, _I, _I, _I, _I, _I, _P]
     L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
     L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
     L.psdm_fd_coef.restype = None

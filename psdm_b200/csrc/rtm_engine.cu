@@ -43,9 +43,9 @@ int fail(int code, const char* fmt, ...) {
                         "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__);    \
     } while (0)
 
-#define TRY(expr)                  \
-    do {                           \
-        int r_ = (expr);           \
+#define TRY(expr)                     \
+    do {                              \
+        int r_ = (expr);              \
         if (r_ != PSDM_OK) return r_; \
     } while (0)
 
@@ -53,18 +53,31 @@ int fail(int code, const char* fmt, ...) {
 
 struct psdm_engine {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;  // own_stream or the caller's
     struct Buf {
         void* ptr = nullptr;
         size_t bytes = 0;
     };
     std::map<std::string, Buf> bufs;
+    // statistics
+    int64_t launches = 0;
+    int64_t fwd_steps = 0, bwd_steps = 0;
+    bool profiling = false;
+    std::vector<cudaEvent_t> events;  // triples (start, forward done, backward done)
+    size_t events_used = 0;
+    // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
+    std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
     // Grow-only named device buffer.
     int get(const char* name, size_t bytes, void** out) {
         Buf& b = bufs[name];
         if (b.bytes < bytes) {
-            if (b.ptr) CUDA_TRY(cudaFree(b.ptr));
+            if (b.ptr) {
+                CUDA_TRY(cudaStreamSynchronize(stream));
+                CUDA_TRY(cudaFree(b.ptr));
+            }
             b.ptr = nullptr;
             b.bytes = 0;
             CUDA_TRY(cudaMalloc(&b.ptr, std::max<size_t>(bytes, 256)));
@@ -88,6 +101,20 @@ struct psdm_engine {
         bufs.clear();
         return PSDM_OK;
     }
+    // Profiling marks: 0 = shot start, 1 = forward done, 2 = backward done.
+    int record(int which) {
+        if (!profiling) return PSDM_OK;
+        if (which == 0 && events_used + 3 > events.size())
+            for (int i = 0; i < 3; ++i) {
+                cudaEvent_t ev;
+                CUDA_TRY(cudaEventCreate(&ev));
+                events.push_back(ev);
+            }
+        const size_t idx = (which == 0) ? events_used : events_used - 3 + which;
+        CUDA_TRY(cudaEventRecord(events[idx], stream));
+        if (which == 0) events_used += 3;
+        return PSDM_OK;
+    }
 };
 
 namespace {
@@ -107,6 +134,10 @@ struct Shot {
     float* fA = nullptr;
     float* fB = nullptr;
     float cf1[4], cf2[4];
+    float inv_dt = 0.f, div_lo = 0.f, div_hi = 0.f, div_tiny = 0.f;
+    int fast_div = 0;
+    int* counters = nullptr;  // two tile counters, alternating per step
+    int num_sms = 0;
 };
 
 // Injection map (sources or adjoint sources at receivers), last write wins
@@ -134,11 +165,26 @@ int build_grid(const psdm_params* prm, int ny, int nx, Grid* g) {
     g->dn = prm->dPML + 2 * kAcc;
     g->nyt = g->dn + ny + g->dn;
     g->nxt = nx + 2 * g->dn;
-    g->ldz = (g->nyt + 31) / 32 * 32;
+    g->zoff = (4 - g->dn % 4) % 4;
+    g->ldz = (g->zoff + g->nyt + 31) / 32 * 32;
+    g->ldf = (ny + 3) / 4 * 4;
     return PSDM_OK;
 }
 
-int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd, float dt, const float* h_vp,
+// Zero the wavefield, memory variables and free-surface histories.
+int reset_state(psdm_engine* e, Shot* s) {
+    const size_t n = s->g.cells();
+    for (float* b : {s->p[0], s->p[1], s->phx[0], s->phx[1], s->chx, s->phz[0], s->phz[1], s->chz})
+        CUDA_TRY(cudaMemsetAsync(b, 0, n * sizeof(float), e->stream));
+    CUDA_TRY(cudaMemsetAsync(s->side[0], 0, s->g.nxt * sizeof(float), e->stream));
+    CUDA_TRY(cudaMemsetAsync(s->side[1], 0, s->g.nxt * sizeof(float), e->stream));
+    CUDA_TRY(cudaMemsetAsync(s->counters, 0, 2 * sizeof(int), e->stream));
+    return PSDM_OK;
+}
+
+// Allocate and initialise the state of a shot from a window model already in
+// device memory (d_vp, (ny, nx) column-major).
+int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd, float dt, const float* d_vp,
                Shot* s) {
     TRY(build_grid(prm, ny, nx, &s->g));
     const Grid& g = s->g;
@@ -165,25 +211,42 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
     TRY(e->get("side1", (size_t)g.nxt, &s->side[1]));
     TRY(e->get("fA", (size_t)g.dn, &s->fA));
     TRY(e->get("fB", (size_t)g.dn, &s->fB));
-    float* d_vp = nullptr;
-    TRY(e->get("vp", (size_t)ny * nx, &d_vp));
+    TRY(e->get("tile_counters", 2, &s->counters));
+    s->num_sms = e->num_sms;
 
     std::vector<float> fA(g.dn), fB(g.dn);
     pml_profiles_f32(kAcc, g.dPML, dt, dd, g.dn, fA.data(), fB.data());
     psdm_fd_coef(1, kAcc, s->cf1);
     psdm_fd_coef(2, kAcc, s->cf2);
+    auto it = e->div_cache.find(dt);
+    if (it == e->div_cache.end()) {
+        float r = 0.f, lo = 0.f, hi = 0.f, tiny = 0.f;
+        const int ok = fast_div_exact(dt, &r, &lo, &hi, &tiny) ? 1 : 0;
+        it = e->div_cache.emplace(dt, std::make_pair(ok, std::vector<float>{r, lo, hi, tiny})).first;
+    }
+    s->fast_div = it->second.first;
+    s->inv_dt = it->second.second[0];
+    s->div_lo = it->second.second[1];
+    s->div_hi = it->second.second[2];
+    s->div_tiny = it->second.second[3];
 
-    cudaStream_t st = e->stream;
-    CUDA_TRY(cudaMemcpyAsync(s->fA, fA.data(), g.dn * sizeof(float), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(s->fB, fB.data(), g.dn * sizeof(float), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(d_vp, h_vp, (size_t)ny * nx * sizeof(float), cudaMemcpyHostToDevice, st));
-    for (float* b : {s->p[0], s->p[1], s->phx[0], s->phx[1], s->chx, s->phz[0], s->phz[1], s->chz})
-        CUDA_TRY(cudaMemsetAsync(b, 0, n * sizeof(float), st));
-    CUDA_TRY(cudaMemsetAsync(s->side[0], 0, g.nxt * sizeof(float), st));
-    CUDA_TRY(cudaMemsetAsync(s->side[1], 0, g.nxt * sizeof(float), st));
-    int rc = launch_pad_c2(d_vp, ny, nx, g.dn, g.nyt, g.nxt, g.ldz, dt, dd, s->disk ? 0 : 1, s->c2, st);
+    CUDA_TRY(cudaMemcpyAsync(s->fA, fA.data(), g.dn * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->fB, fB.data(), g.dn * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    TRY(reset_state(e, s));
+    int rc = launch_pad_c2(d_vp, ny, nx, g.dn, g.nyt, g.nxt, g.ldz, g.zoff, dt, dd, s->disk ? 0 : 1, s->c2,
+                           e->stream);
     if (rc) return fail(PSDM_ERR_CUDA, "pad_c2 launch: %s", cudaGetErrorString((cudaError_t)rc));
+    e->launches += 1;
     return PSDM_OK;
+}
+
+// Same, uploading the window model from host memory first.
+int setup_shot_host(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd, float dt, const float* h_vp,
+                    Shot* s) {
+    float* d_vp = nullptr;
+    TRY(e->get("vp", (size_t)ny * nx, &d_vp));
+    CUDA_TRY(cudaMemcpyAsync(d_vp, h_vp, (size_t)ny * nx * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    return setup_shot(e, prm, ny, nx, dd, dt, d_vp, s);
 }
 
 // zs/xs: padded 0-based coordinates.  Points outside the padded grid are an
@@ -191,7 +254,7 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
 // kept out of the map because the reference adds `source` only on the
 // interior (solver_ac_forward_ram.f90:443-444).
 int build_inj(const Grid& g, int n, const int* zs, const int* xs, InjMap* m) {
-    m->row_slot.assign(g.nyt, -1);
+    m->row_slot.assign(g.ldz, -1);
     m->cols.clear();
     m->nslots = 0;
     for (int j = 0; j < n; ++j) {
@@ -200,19 +263,23 @@ int build_inj(const Grid& g, int n, const int* zs, const int* xs, InjMap* m) {
             return fail(PSDM_ERR_ARG, "injection point %d at padded (z=%d, x=%d) lies outside the %dx%d grid", j, z,
                         x, g.nyt, g.nxt);
         if (z < g.dn || z >= g.dn + g.ny || x < g.dn || x >= g.dn + g.nx) continue;
-        if (m->row_slot[z] < 0) {
-            m->row_slot[z] = m->nslots++;
+        const int zd = z + g.zoff;
+        if (m->row_slot[zd] < 0) {
+            m->row_slot[zd] = m->nslots++;
             m->cols.resize((size_t)m->nslots * g.nxt, -1);
         }
-        m->cols[(size_t)m->row_slot[z] * g.nxt + x] = j;
+        m->cols[(size_t)m->row_slot[zd] * g.nxt + x] = j;
     }
     return PSDM_OK;
 }
 
-int upload_inj(psdm_engine* e, const Grid& g, const InjMap& m, int** d_row, int** d_cols) {
-    TRY(e->get("inj_row", (size_t)g.nyt, d_row));
-    TRY(e->get("inj_cols", std::max<size_t>(m.cols.size(), 1), d_cols));
-    CUDA_TRY(cudaMemcpyAsync(*d_row, m.row_slot.data(), g.nyt * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+// Pageable-host sources are staged by cudaMemcpyAsync before it returns, so
+// the vectors may be released right after.
+int upload_inj(psdm_engine* e, const Grid& g, const InjMap& m, const char* tag, int** d_row, int** d_cols) {
+    const std::string rn = std::string("inj_row_") + tag, cn = std::string("inj_cols_") + tag;
+    TRY(e->get(rn.c_str(), (size_t)g.ldz, d_row));
+    TRY(e->get(cn.c_str(), std::max<size_t>(m.cols.size(), 1), d_cols));
+    CUDA_TRY(cudaMemcpyAsync(*d_row, m.row_slot.data(), g.ldz * sizeof(int), cudaMemcpyHostToDevice, e->stream));
     if (!m.cols.empty())
         CUDA_TRY(cudaMemcpyAsync(*d_cols, m.cols.data(), m.cols.size() * sizeof(int), cudaMemcpyHostToDevice,
                                  e->stream));
@@ -229,9 +296,19 @@ StepArgs base_args(const Shot& s) {
     a.fB = s.fB;
     for (int i = 0; i < 4; ++i) { a.cf1[i] = s.cf1[i]; a.cf2[i] = s.cf2[i]; }
     a.nyt = s.g.nyt; a.nxt = s.g.nxt; a.ldz = s.g.ldz; a.ny = s.g.ny; a.nx = s.g.nx; a.dn = s.g.dn;
+    a.zoff = s.g.zoff; a.ldf = s.g.ldf;
+    a.fs = s.fs;
+    plan_tiles(&a);
+    a.tile_counter = s.counters;
+    a.num_sms = s.num_sms;
     a.fs = s.fs;
     a.disk = s.disk;
     a.dt = s.dt;
+    a.inv_dt = s.inv_dt;
+    a.div_lo = s.div_lo;
+    a.div_hi = s.div_hi;
+    a.div_tiny = s.div_tiny;
+    a.fast_div = s.fast_div;
     a.rec_t = -1;
     a.ss = 1.f;
     a.field_w = 1.f;
@@ -241,6 +318,7 @@ StepArgs base_args(const Shot& s) {
 // Rotate ping-pong pointers for step number `it` (0 for k = 2).
 void set_buffers(const Shot& s, int it, StepArgs* a) {
     const int c = it & 1;
+    a->counter_sel = c;
     a->p = s.p[c];
     a->pm = s.p[c ^ 1];
     a->phix_in = s.phx[c];
@@ -260,7 +338,7 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     InjMap inj;
     TRY(build_inj(g, 1, &zs, &xs, &inj));
     int *d_row = nullptr, *d_cols = nullptr;
-    TRY(upload_inj(e, g, inj, &d_row, &d_cols));
+    TRY(upload_inj(e, g, inj, "src", &d_row, &d_cols));
     int* d_rec_cell = nullptr;
     if (d_rec && nrec > 0) {
         TRY(e->get("rec_cell", (size_t)nrec, &d_rec_cell));
@@ -276,11 +354,11 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     a.rec_out = d_rec;
     a.nrec = d_rec ? nrec : 0;
     a.rec_ld = nt;
-    const size_t fstride = (size_t)g.ny * g.nx;
+    const size_t fstride = g.field_cells();
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
-        a.inj_t = k - 2;                        // S(k-1)
+        a.inj_t = k - 2;                           // S(k-1)
         a.rec_t = (d_rec && k >= 3) ? k - 3 : -1;  // Rec(k-2) from p = level k-1
         a.field = nullptr;
         if (d_fields && (k - 1) % store_snap == 0) {
@@ -291,27 +369,32 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
         int rc = launch_step(0, a, e->stream);
         if (rc) return fail(PSDM_ERR_CUDA, "forward step %d: %s", k, cudaGetErrorString((cudaError_t)rc));
     }
+    e->launches += nt - 1;
+    e->fwd_steps += nt - 1;
     if (d_rec && nrec > 0 && nt >= 2) {
         const float* pfin = s.p[(nt - 1) & 1];  // p3 of the last step
         int rc = launch_rec_final(d_rec_cell, pfin, d_rec, nrec, nt, nt, e->stream);
         if (rc) return fail(PSDM_ERR_CUDA, "receiver gather: %s", cudaGetErrorString((cudaError_t)rc));
+        e->launches += 1;
     }
     return PSDM_OK;
 }
 
 // Backward pass over k = 2..nt (solver_ac_backward_ram.f90:329-545).
-//   d_back: adjoint traces (nt, NumRec); snapshots: slot `snap` (1-based) is
-//   d_fields + (snap - slot_lo) * ny*nx when slot_lo <= snap <= slot_hi, and
-//   zero otherwise; h_w[snap - 1] is the taper weight of slot `snap`
-//   (size nt_snap, may be null for all-ones).
-int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int nrec,
-                 const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
+//   d_back: adjoint traces (nt, NumRec); with reverse = 1 they are read in
+//   reverse time order, which is BackSource(:,j) = Data_target(nt:1:-1, j)
+//   (calculate_PSDM_RTM.f90:448-450) without materialising it.
+//   Snapshots: slot `snap` (1-based) is d_fields + (snap - slot_lo) * ny*nx
+//   when slot_lo <= snap <= slot_hi, and zero otherwise; h_w[snap - 1] is the
+//   taper weight of slot `snap` (size >= nt_snap; null for all ones).
+int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
+                 int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
                  const float* h_w, float* d_image) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, nrec, zr, xr, &inj));
     int *d_row = nullptr, *d_cols = nullptr;
-    TRY(upload_inj(e, g, inj, &d_row, &d_cols));
+    TRY(upload_inj(e, g, inj, "rec", &d_row, &d_cols));
     StepArgs a = base_args(s);
     a.row_slot = d_row;
     a.inj_cols = d_cols;
@@ -319,12 +402,12 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
     a.inj_ld = nt;
     a.image = d_image;
     a.ss = float(store_snap);
-    const size_t fstride = (size_t)g.ny * g.nx;
+    const size_t fstride = g.field_cells();
     int snap = nt_snap;
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
-        a.inj_t = k - 2;  // Sadj(k-1)
+        a.inj_t = reverse ? nt - k + 1 : k - 2;  // Sadj(k-1)
         a.field = nullptr;
         if ((k - 1) % store_snap == 0) {
             snap = snap - 1;
@@ -337,6 +420,8 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
         int rc = launch_step(1, a, e->stream);
         if (rc) return fail(PSDM_ERR_CUDA, "backward step %d: %s", k, cudaGetErrorString((cudaError_t)rc));
     }
+    e->launches += nt - 1;
+    e->bwd_steps += nt - 1;
     return PSDM_OK;
 }
 
@@ -355,9 +440,9 @@ int sync(psdm_engine* e) {
 // src/dynamic_window.f90:80-86): x_i from the model-coordinate geometry.
 struct WinGeom {
     int x_i = 1, nx_w_calc = 0;
-    int zs = 0, xs = 0;               // padded 0-based source
-    std::vector<int> zr, xr;          // padded 0-based receivers
-    std::vector<int> rec_cell;        // xr*ldz + zr
+    int zs = 0, xs = 0;         // padded 0-based source (logical rows)
+    std::vector<int> zr, xr;    // padded 0-based receivers (logical rows)
+    std::vector<int> rec_cell;  // xr*ldz + zr + zoff
 };
 
 int window_geometry(const Grid& g, int NumRec, int nxSou, int nySou, const int* nxRec, const int* nyRec, float dd,
@@ -377,8 +462,59 @@ int window_geometry(const Grid& g, int NumRec, int nxSou, int nySou, const int* 
         if (w->zr[r] < 0 || w->zr[r] >= g.nyt || w->xr[r] < 0 || w->xr[r] >= g.nxt)
             return fail(PSDM_ERR_ARG, "receiver %d at padded (z=%d, x=%d) lies outside the %dx%d grid", r, w->zr[r],
                         w->xr[r], g.nyt, g.nxt);
-        w->rec_cell[r] = w->xr[r] * g.ldz + w->zr[r];
+        w->rec_cell[r] = w->xr[r] * g.ldz + w->zr[r] + g.zoff;
     }
+    return PSDM_OK;
+}
+
+// One shot of RTM with every array in device memory
+// (calculate_PSDM_RTM.f90:395-466).  Asynchronous on e->stream.
+int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
+                  const int* nyRec, const float* d_S, const float* d_tgt, float dd, float dt, int ny, int nx,
+                  int nx_w, const float* d_vp, float added_space, int store_snap, int nt_snap, int nt_prop2,
+                  int nt_taper, int taper_option, int N_taper, int N_zeros, float* d_img) {
+    TRY(check_params(prm));
+    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (NumRec < 1 || !nxRec || !nyRec || !d_S || !d_tgt || !d_vp || !d_img)
+        return fail(PSDM_ERR_ARG, "null argument or NumRec < 1");
+    if (nt_prop2 < 2 || nt_taper < 2 || store_snap < 1 || nt_taper < nt_prop2)
+        return fail(PSDM_ERR_ARG, "need 2 <= nt_prop2 <= nt_taper and store_snap >= 1");
+    if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
+    const int nsnap = (nt_prop2 - 1) / store_snap;  // slots written by the forward pass
+    if (nsnap > nt_snap) return fail(PSDM_ERR_ARG, "nt_snap=%d < %d snapshots", nt_snap, nsnap);
+    Shot s;
+    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &s));
+    WinGeom w;
+    TRY(window_geometry(s.g, NumRec, nxSou, nySou, nxRec, nyRec, dd, nx, added_space, &w));
+    if (w.nx_w_calc != nx_w)
+        return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
+    const size_t fstride = s.g.field_cells();
+    float *d_F = nullptr, *d_imgp = nullptr;
+    if (nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
+    TRY(e->get("image_pitched", fstride, &d_imgp));
+    TRY(e->record(0));
+    TRY(run_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr));
+    TRY(e->record(1));
+
+    // Taper of the snapshot series (calculate_PSDM_RTM.f90:421-427): a weight
+    // per slot, applied when the slot is read.
+    std::vector<float> wts(std::max(nt_taper, 1), 1.f);
+    if (taper_option != 0) {
+        const int i0 = std::max(1, nt_prop2 - N_taper + 1);
+        for (int n = 0; n < N_taper; ++n)
+            if (i0 + n <= nt_prop2) wts[i0 + n - 1] = taper_weight(n, N_taper);
+        if (N_zeros > 0)
+            for (int i = nt_prop2; i < nt_taper; ++i) wts[i] = 0.f;
+    }
+    CUDA_TRY(cudaMemsetAsync(d_imgp, 0, fstride * sizeof(float), e->stream));
+    // Second propagator call: nt_snap = nt = nt_taper (:456-458); same model.
+    TRY(reset_state(e, &s));
+    TRY(run_backward(e, s, nt_taper, store_snap, nt_taper, d_tgt, 1, NumRec, w.zr.data(), w.xr.data(), d_F, 1,
+                     nsnap, wts.data(), d_imgp));
+    TRY(e->record(2));
+    // Pitched interior image -> caller's (ny, nx_w) image.
+    CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
+                               (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
     return PSDM_OK;
 }
 
@@ -400,11 +536,13 @@ int psdm_engine_create(int32_t device, psdm_engine** out) {
     CUDA_TRY(cudaSetDevice(device));
     psdm_engine* e = new psdm_engine();
     e->device = device;
-    err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device);
+    err = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
     if (err != cudaSuccess) {
         delete e;
         return fail(PSDM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(err));
     }
+    e->stream = e->own_stream;
     *out = e;
     return PSDM_OK;
 }
@@ -414,9 +552,55 @@ int psdm_engine_destroy(psdm_engine* e) {
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     int rc = e->trim();
-    cudaStreamDestroy(e->stream);
+    for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
+    cudaStreamDestroy(e->own_stream);
     delete e;
     return rc;
+}
+
+int psdm_engine_set_stream(psdm_engine* e, void* stream) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    e->stream = stream ? (cudaStream_t)stream : e->own_stream;
+    return PSDM_OK;
+}
+
+int psdm_engine_set_profiling(psdm_engine* e, int32_t on) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    e->profiling = on != 0;
+    e->events_used = 0;
+    return PSDM_OK;
+}
+
+int psdm_engine_stats(psdm_engine* e, psdm_stats* out) {
+    TRY(check_engine(e));
+    if (!out) return fail(PSDM_ERR_ARG, "out is NULL");
+    TRY(sync(e));
+    std::memset(out, 0, sizeof(*out));
+    out->launches = e->launches;
+    out->fwd_steps = e->fwd_steps;
+    out->bwd_steps = e->bwd_steps;
+    double f = 0.0, b = 0.0;
+    for (size_t i = 0; i + 3 <= e->events_used; i += 3) {
+        float t1 = 0.f, t2 = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&t1, e->events[i], e->events[i + 1]));
+        CUDA_TRY(cudaEventElapsedTime(&t2, e->events[i + 1], e->events[i + 2]));
+        f += t1;
+        b += t2;
+        out->shots += 1;
+    }
+    out->fwd_ms = f;
+    out->bwd_ms = b;
+    return PSDM_OK;
+}
+
+int psdm_engine_reset_stats(psdm_engine* e) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    e->launches = e->fwd_steps = e->bwd_steps = 0;
+    e->events_used = 0;
+    return PSDM_OK;
 }
 
 int64_t psdm_engine_device_bytes(const psdm_engine* e) { return e ? e->total() : 0; }
@@ -440,7 +624,7 @@ int psdm_dynamic_window_solver_forward_ram(psdm_engine* e, const psdm_params* pr
         return fail(PSDM_ERR_ARG, "null argument");
     if (nt < 2 || store_snap < 1 || nt_snap < 0) return fail(PSDM_ERR_ARG, "need nt >= 2, store_snap >= 1");
     Shot s;
-    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
+    TRY(setup_shot_host(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
     WinGeom w;
     TRY(window_geometry(s.g, NumRec, nxSou[0], nySou[0], nxRec, nyRec, dd, nx, dd_space, &w));
     if (w.nx_w_calc != nx_w)
@@ -450,12 +634,13 @@ int psdm_dynamic_window_solver_forward_ram(psdm_engine* e, const psdm_params* pr
     CUDA_TRY(cudaMemcpyAsync(d_S, Data_source, nt * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     const int nsnap = (nt - 1) / store_snap;
     if (Fields && nsnap > nt_snap) return fail(PSDM_ERR_ARG, "nt_snap=%d < %d snapshots", nt_snap, nsnap);
-    const size_t fstride = (size_t)ny * nx_w;
-    if (Fields && nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
+    if (Fields && nsnap > 0) TRY(e->get("fields", s.g.field_cells() * nsnap, &d_F));
     if (Data_synth && NumRec > 0) TRY(e->get("rec", (size_t)NumRec * nt, &d_rec));
     TRY(run_forward(e, s, nt, store_snap, d_S, w.zs, w.xs, d_F, nsnap, NumRec, w.rec_cell.data(), d_rec));
-    if (d_F)
-        CUDA_TRY(cudaMemcpyAsync(Fields, d_F, fstride * nsnap * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    if (d_F)  // pitched columns (ldf) -> dense Fields(ny, nx_w, slot)
+        CUDA_TRY(cudaMemcpy2DAsync(Fields, (size_t)ny * sizeof(float), d_F, (size_t)s.g.ldf * sizeof(float),
+                                   (size_t)ny * sizeof(float), (size_t)nx_w * nsnap, cudaMemcpyDeviceToHost,
+                                   e->stream));
     if (d_rec)
         CUDA_TRY(cudaMemcpyAsync(Data_synth, d_rec, (size_t)NumRec * nt * sizeof(float), cudaMemcpyDeviceToHost,
                                  e->stream));
@@ -475,17 +660,18 @@ int psdm_dynamic_window_solver_backward_ram(psdm_engine* e, const psdm_params* p
         return fail(PSDM_ERR_ARG, "null argument");
     if (nt < 2 || store_snap < 1) return fail(PSDM_ERR_ARG, "need nt >= 2, store_snap >= 1");
     Shot s;
-    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
+    TRY(setup_shot_host(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
     WinGeom w;
     TRY(window_geometry(s.g, NumRec, nxSou[0], nySou[0], nxRec, nyRec, dd, nx, dd_space, &w));
     if (w.nx_w_calc != nx_w)
         return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
-    // Slots read: nt_snap - m for m = 1..(nt-1)/store_snap, clipped to [1, nt_snap].
+    // Slots read: nt_snap - m for m = 1..(nt-1)/store_snap.
     const int nimg = (nt - 1) / store_snap;
-    const int lo = std::max(1, nt_snap - nimg), hi = nt_snap - 1;
-    if (nt_snap - nimg < 1 && nimg > 0 && Fields)
-        return fail(PSDM_ERR_ARG, "imaging would read snapshot slot %d < 1 (nt_snap=%d)", nt_snap - nimg, nt_snap);
-    const size_t fstride = (size_t)ny * nx_w;
+    const int lo = nt_snap - nimg, hi = nt_snap - 1;
+    if (lo < 1 && nimg > 0 && Fields)
+        return fail(PSDM_ERR_ARG, "imaging would read snapshot slot %d < 1 (nt_snap=%d)", lo, nt_snap);
+    const size_t hstride = (size_t)ny * nx_w;  // dense host slot
+    const size_t ld = (size_t)s.g.ldf * sizeof(float), wb = (size_t)ny * sizeof(float);
     float *d_back = nullptr, *d_F = nullptr, *d_img = nullptr;
     if (NumRec > 0) {
         TRY(e->get("back", (size_t)NumRec * nt, &d_back));
@@ -493,15 +679,15 @@ int psdm_dynamic_window_solver_backward_ram(psdm_engine* e, const psdm_params* p
                                  e->stream));
     }
     if (Fields && hi >= lo) {
-        TRY(e->get("fields", fstride * (hi - lo + 1), &d_F));
-        CUDA_TRY(cudaMemcpyAsync(d_F, Fields + (size_t)(lo - 1) * fstride, fstride * (hi - lo + 1) * sizeof(float),
-                                 cudaMemcpyHostToDevice, e->stream));
+        TRY(e->get("fields", s.g.field_cells() * (hi - lo + 1), &d_F));
+        CUDA_TRY(cudaMemcpy2DAsync(d_F, ld, Fields + (size_t)(lo - 1) * hstride, wb, wb, (size_t)nx_w * (hi - lo + 1),
+                                   cudaMemcpyHostToDevice, e->stream));
     }
-    TRY(e->get("image", fstride, &d_img));
-    CUDA_TRY(cudaMemcpyAsync(d_img, PSDM_thread, fstride * sizeof(float), cudaMemcpyHostToDevice, e->stream));
-    TRY(run_backward(e, s, nt, store_snap, nt_snap, d_back, NumRec, w.zr.data(), w.xr.data(), d_F, lo, hi, nullptr,
-                     d_img));
-    CUDA_TRY(cudaMemcpyAsync(PSDM_thread, d_img, fstride * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    TRY(e->get("image_pitched", s.g.field_cells(), &d_img));
+    CUDA_TRY(cudaMemcpy2DAsync(d_img, ld, PSDM_thread, wb, wb, nx_w, cudaMemcpyHostToDevice, e->stream));
+    TRY(run_backward(e, s, nt, store_snap, nt_snap, d_back, 0, NumRec, w.zr.data(), w.xr.data(), d_F, lo, hi,
+                     nullptr, d_img));
+    CUDA_TRY(cudaMemcpy2DAsync(PSDM_thread, wb, d_img, ld, wb, nx_w, cudaMemcpyDeviceToHost, e->stream));
     return sync(e);
 }
 
@@ -511,52 +697,35 @@ int psdm_rtm_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_
                   int32_t store_snap, int32_t nt_snap, int32_t nt_prop2, int32_t nt_taper, int32_t taper_option,
                   int32_t N_taper, int32_t N_zeros, float* PSDM_w) {
     TRY(check_engine(e));
-    TRY(check_params(prm));
-    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
-    if (NumRec < 1 || !nxRec || !nyRec || !Data_source || !Data_target || !Vp_w || !PSDM_w)
-        return fail(PSDM_ERR_ARG, "null argument or NumRec < 1");
-    if (nt_prop2 < 2 || nt_taper < 2 || store_snap < 1 || nt_taper < nt_prop2)
-        return fail(PSDM_ERR_ARG, "need 2 <= nt_prop2 <= nt_taper and store_snap >= 1");
-    if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
-    Shot s;
-    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
-    WinGeom w;
-    TRY(window_geometry(s.g, NumRec, nxSou, nySou, nxRec, nyRec, dd, nx, added_space, &w));
-    if (w.nx_w_calc != nx_w)
-        return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
+    if (!Data_source || !Data_target || !Vp_w || !PSDM_w || NumRec < 1 || nt_prop2 < 1 || nt_taper < 1 || ny < 1 ||
+        nx_w < 1)
+        return fail(PSDM_ERR_ARG, "null argument or empty size");
     const size_t fstride = (size_t)ny * nx_w;
-    const int nsnap = (nt_prop2 - 1) / store_snap;  // slots written by the forward pass
-    float *d_S = nullptr, *d_F = nullptr, *d_back = nullptr, *d_img = nullptr;
+    float *d_vp = nullptr, *d_S = nullptr, *d_tgt = nullptr, *d_img = nullptr;
+    TRY(e->get("vp", fstride, &d_vp));
     TRY(e->get("S", (size_t)nt_prop2, &d_S));
-    CUDA_TRY(cudaMemcpyAsync(d_S, Data_source, nt_prop2 * sizeof(float), cudaMemcpyHostToDevice, e->stream));
-    if (nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
-    TRY(run_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr));
-
-    // Taper of the snapshot series (calculate_PSDM_RTM.f90:421-427): a weight
-    // per slot, applied when the slot is read.
-    std::vector<float> wts(std::max(nt_taper, 1), 1.f);
-    if (taper_option != 0) {
-        const int i0 = std::max(1, nt_prop2 - N_taper + 1);
-        for (int n = 0; n < N_taper; ++n)
-            if (i0 + n <= nt_prop2) wts[i0 + n - 1] = taper_weight(n, N_taper);
-        if (N_zeros > 0)
-            for (int i = nt_prop2; i < nt_taper; ++i) wts[i] = 0.f;
-    }
-    // BackSource(:,j) = Data_target(nt_taper:1:-1, j) (:448-450).
-    std::vector<float> back((size_t)NumRec * nt_taper);
-    for (int r = 0; r < NumRec; ++r)
-        for (int t = 0; t < nt_taper; ++t)
-            back[(size_t)r * nt_taper + t] = Data_target[(size_t)r * nt_taper + (nt_taper - 1 - t)];
-    TRY(e->get("back", back.size(), &d_back));
-    CUDA_TRY(cudaMemcpyAsync(d_back, back.data(), back.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    TRY(e->get("tgt", (size_t)NumRec * nt_taper, &d_tgt));
     TRY(e->get("image", fstride, &d_img));
-    CUDA_TRY(cudaMemsetAsync(d_img, 0, fstride * sizeof(float), e->stream));
-    // Second propagator call: nt_snap = nt = nt_taper (:456-458).
-    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
-    TRY(run_backward(e, s, nt_taper, store_snap, nt_taper, d_back, NumRec, w.zr.data(), w.xr.data(), d_F, 1, nsnap,
-                     wts.data(), d_img));
+    CUDA_TRY(cudaMemcpyAsync(d_vp, Vp_w, fstride * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_S, Data_source, nt_prop2 * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_tgt, Data_target, (size_t)NumRec * nt_taper * sizeof(float), cudaMemcpyHostToDevice,
+                             e->stream));
+    TRY(rtm_shot_core(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_S, d_tgt, dd, dt, ny, nx, nx_w, d_vp, added_space,
+                      store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, d_img));
     CUDA_TRY(cudaMemcpyAsync(PSDM_w, d_img, fstride * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
     return sync(e);
+}
+
+int psdm_rtm_shot_device(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+                         const int32_t* nxRec, const int32_t* nyRec, const float* d_Data_source,
+                         const float* d_Data_target, float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w,
+                         const float* d_Vp_w, float added_space, int32_t store_snap, int32_t nt_snap,
+                         int32_t nt_prop2, int32_t nt_taper, int32_t taper_option, int32_t N_taper, int32_t N_zeros,
+                         float* d_PSDM_w) {
+    TRY(check_engine(e));
+    return rtm_shot_core(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_Data_source, d_Data_target, dd, dt, ny, nx,
+                         nx_w, d_Vp_w, added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper,
+                         N_zeros, d_PSDM_w);
 }
 
 int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
@@ -569,7 +738,7 @@ int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int3
         return fail(PSDM_ERR_ARG, "null argument or NumRec < 1");
     if (nt < 2) return fail(PSDM_ERR_ARG, "need nt >= 2");
     Shot s;
-    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
+    TRY(setup_shot_host(e, prm, ny, nx_w, dd, dt, Vp_w, &s));
     WinGeom w;
     TRY(window_geometry(s.g, NumRec, nxSou, nySou, nxRec, nyRec, dd, nx, dd_space, &w));
     if (w.nx_w_calc != nx_w)

@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "../../include/psdm_rtm.h"
@@ -55,6 +57,36 @@ void pml_profiles_f64(int acc, int dPML, double dt, double d, int dn, double* fA
         fB[i - 1] = ((A - 1.0) * sigma) / (sigma + alpha);
     }
     for (int i = dPML + acc + 1; i <= dn; ++i) { fA[i - 1] = fA[dPML + acc - 1]; fB[i - 1] = fB[dPML + acc - 1]; }
+}
+
+// Division by a fixed y as q0 = RN(x*r), e = x - q0*y (exact, one FMA),
+// q = RN(q0 + e*r) with r = RN(1/y).  By Markstein's theorem this is the
+// correctly rounded x/y when no intermediate leaves the normal range; the
+// check below confirms it for every significand of one binade of x (the
+// result scales exactly with powers of two of x), so for |x| in [lo, hi]
+// the kernels may use it in place of an IEEE division.
+bool fast_div_exact(float y, float* r, float* lo, float* hi, float* tiny) {
+    volatile float one = 1.0f;
+    const float rr = one / y;
+    *r = rr;
+    *lo = ldexpf(1.0f, -90);
+    *hi = std::min(ldexpf(1.0f, 100), ldexpf(y, 120));
+    // below lo the kernels scale x by 2^64: x*2^64 must stay >= lo, and the
+    // quotient must be normal for the scaling back to be exact
+    *tiny = std::max(ldexpf(1.0f, -154), ldexpf(y, -124));
+    if (!(ldexpf(*tiny, 64) >= *lo)) *tiny = ldexpf(*lo, -64);
+    if (!(y > 0.f) || !std::isfinite(y) || !std::isfinite(rr)) return false;
+    for (uint32_t m = 0; m < (1u << 23); ++m) {
+        const uint32_t bits = 0x3f800000u | m;
+        float x;
+        std::memcpy(&x, &bits, sizeof(x));
+        const float q0 = x * rr;
+        const float e = std::fmaf(-q0, y, x);
+        const float q = std::fmaf(e, rr, q0);
+        volatile float xv = x;
+        if (q != xv / y) return false;
+    }
+    return true;
 }
 
 float taper_weight(int n, int N_taper) {

@@ -12,14 +12,22 @@ constexpr int kAcc = 3;  // FD half-width (acc=3, src/solver_ac_forward_ram.f90:
 void pml_profiles_f32(int acc, int dPML, float dt, float d, int dn, float* fA, float* fB);
 void pml_profiles_f64(int acc, int dPML, double dt, double d, int dn, double* fA, double* fB);
 float taper_weight(int n, int N_taper);
+// True if x/y may be computed as RN(q0 + (x - q0*y)*r), q0 = RN(x*r),
+// r = RN(1/y), for |x| in [lo, hi] (exhaustive check over one binade).
+bool fast_div_exact(float y, float* r, float* lo, float* hi, float* tiny);
 
 // Padded propagation grid of one shot (0-based, column-major, z fastest):
-//   z in [0, nyt), x in [0, nxt), element (z, x) at x*ldz + z.
+//   logical z in [0, nyt), x in [0, nxt); element (z, x) is stored at device
+//   row zd = z + zoff, i.e. at x*ldz + zd.  zoff in [0, 3] makes the first
+//   interior row dn start on a 16-byte boundary.
 // Interior rows [dn, dn+ny), interior columns [dn, dn+nx); dn = dPML+2*acc
 // (src/solver_ac_forward_ram.f90:103-127).
+// Snapshots and images of the interior are stored column by column with the
+// pitch ldf = ny rounded up to 4: interior cell (j, i) at i*ldf + j.
 struct Grid {
-    int ny = 0, nx = 0, dPML = 0, dn = 0, nyt = 0, nxt = 0, ldz = 0;
+    int ny = 0, nx = 0, dPML = 0, dn = 0, nyt = 0, nxt = 0, ldz = 0, zoff = 0, ldf = 0;
     size_t cells() const { return (size_t)ldz * (size_t)nxt; }
+    size_t field_cells() const { return (size_t)ldf * (size_t)nx; }
 };
 
 // Arguments of one fused time step.  Pointers are device pointers.
@@ -46,10 +54,11 @@ struct StepArgs {
     float cf1[4];
     float cf2[4];
     // grid
-    int nyt, nxt, ldz, ny, nx, dn;
+    int nyt, nxt, ldz, ny, nx, dn, zoff, ldf;
     int fs;     // free surface on
     int disk;   // disk solvers' statement order
-    // injection (sources / adjoint sources): row_slot[z] = -1 or a row slot;
+    // injection (sources / adjoint sources): row_slot[zd] = -1 or a row slot
+    // (indexed by device row, ldz entries);
     // inj_cols[slot*nxt + x] = trace index or -1; value inj_trace[j*inj_ld + inj_t]
     const int* row_slot;
     const int* inj_cols;
@@ -58,7 +67,10 @@ struct StepArgs {
     // forward snapshot (write) or backward snapshot (read); null = none this step
     float* field;
     float dt;
-    // backward imaging: image[(x-dn)*ny + (z-dn)] += 0.5*(p3-p1)*field*w*ss
+    // snapshot division by dt: reciprocal + one FMA correction when exact
+    float inv_dt, div_lo, div_hi, div_tiny;
+    int fast_div;
+    // backward imaging: image[(x-dn)*ldf + (z-dn)] += 0.5*(p3-p1)*field*w*ss
     float* image;
     float field_w;   // taper weight of this snapshot slot
     float ss;        // float(store_snap)
@@ -66,7 +78,22 @@ struct StepArgs {
     const int* rec_cell;
     float* rec_out;
     int nrec, rec_ld, rec_t;  // rec_t < 0: no gather this step
+    // block decomposition (plan_tiles): rect r of type r_type (0 interior
+    // band, 1 C-PML x-strip band, 2 z-strip, 3 corner) covers device rows
+    // [r_zd0, r_zd0+r_h) x columns [r_x0, r_x0+r_w); its tiles are blocks
+    // [r_first[r], r_first[r+1]) with r_tz tiles along z.
+    int nrect;
+    int r_type[9], r_zd0[9], r_x0[9], r_h[9], r_w[9], r_tz[9], r_first[10];
+    // persistent scheduling: tile_counter[counter_sel] starts at 0 (cleared
+    // by the previous step); num_sms = multiprocessor count of the device
+    int* tile_counter;
+    int counter_sel;
+    int num_sms;
 };
+
+// Fill the block decomposition of `a` from its grid fields (nyt, nxt, ny,
+// nx, dn, zoff, fs).
+void plan_tiles(StepArgs* a);
 
 // Launch one fused forward (mode 0) or backward (mode 1) step on `stream`.
 int launch_step(int mode, const StepArgs& a, void* stream);
@@ -74,7 +101,7 @@ int launch_step(int mode, const StepArgs& a, void* stream);
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream);
 // Padded c2 = c^2 dt^2 / d^2 from the window model (edge replication;
 // ram_padding = 1 reproduces the RAM solvers' partial top/bottom padding).
-int launch_pad_c2(const float* vp, int ny, int nx, int dn, int nyt, int nxt, int ldz, float dt, float dd,
+int launch_pad_c2(const float* vp, int ny, int nx, int dn, int nyt, int nxt, int ldz, int zoff, float dt, float dd,
                   int ram_padding, float* c2, void* stream);
 
 }  // namespace psdm

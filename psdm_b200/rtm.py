@@ -69,6 +69,21 @@ class Engine:
         except Exception:
             pass
 
+    def set_stream(self, stream_ptr: int | None):
+        """Queue work on a caller's cudaStream_t (e.g. torch's current stream)."""
+        L.check(L.lib().psdm_engine_set_stream(self._h, stream_ptr))
+
+    def set_profiling(self, on: bool):
+        L.check(L.lib().psdm_engine_set_profiling(self._h, int(on)))
+
+    def stats(self) -> dict:
+        st = L.Stats()
+        L.check(L.lib().psdm_engine_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in L.Stats._fields_}
+
+    def reset_stats(self):
+        L.check(L.lib().psdm_engine_reset_stats(self._h))
+
     def device_bytes(self) -> int:
         return int(L.lib().psdm_engine_device_bytes(self._h))
 
@@ -128,6 +143,16 @@ class Engine:
             _f32(Data_source).reshape(-1), tgt.reshape(-1), dd, dt, ny, nx, nx_w, _f32(Vp_w), added_space,
             store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, PSDM_w))
         return PSDM_w
+
+    def rtm_shot_device(self, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, d_Data_source: int,
+                        d_Data_target: int, dd, dt, ny, nx, nx_w, d_Vp_w: int, added_space, store_snap, nt_snap,
+                        nt_prop2, nt_taper, taper_option, N_taper, N_zeros, d_PSDM_w: int):
+        """psdm_rtm_shot_device: d_* are device pointers (ints); asynchronous."""
+        nxRec = _i32(nxRec)
+        L.check(L.lib().psdm_rtm_shot_device(
+            self._h, C.byref(prm.c()), nxRec.size, int(nxSou), int(nySou), nxRec, _i32(nyRec), d_Data_source,
+            d_Data_target, dd, dt, ny, nx, nx_w, d_Vp_w, added_space, store_snap, nt_snap, nt_prop2, nt_taper,
+            taper_option, N_taper, N_zeros, d_PSDM_w))
 
     def model_shot(self, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, dd, dt, ny, nx, nx_w,
                    Vp_w, dd_space, nt):

@@ -122,3 +122,22 @@ def test_rejects_geometry_outside_grid(engine):
     with pytest.raises(PsdmError):
         engine.model_shot(_prm(c), c["nxSou"], c["nySou"], c["nxRec"], bad, c["src"], c["dd"], c["dt"], c["ny"],
                           c["nx"], c["nx_w"], c["vp_w"], c["added_space"], c["nt"])
+
+
+@pytest.mark.parametrize("dPML,fs,strategy", [(8, 1, 1), (11, 0, 2), (20, 1, 2)])
+def test_rtm_shot_multi_tile_exact(engine, oracle, dPML, fs, strategy):
+    """Windows spanning several 128x32 tiles, including dn not a multiple of 4."""
+    c = make_case(ny=150, nx_model=420, nt=90, dPML=dPML, fs=fs, strategy=strategy, nrec=60, rec_step=3,
+                  sou_x=300, sou_z=5, rec_z=3, added_space=150.0, seed=31 + dPML)
+    img_o = oracle.rtm_shot(dPML=c["dPML"], fs=c["fs"], nxSou=c["nxSou"], nySou=c["nySou"], nxRec=c["nxRec"],
+                            nyRec=c["nyRec"], Data_source=c["src"], Data_target=c["tgt"], dd=c["dd"], dt=c["dt"],
+                            nx=c["nx"], vp_w=c["vp_w"], added_space=c["added_space"], store_snap=1,
+                            nt_snap=c["nt"], nt_prop2=c["nt"], nt_taper=c["nt"], disk_mode=int(strategy == 2))
+    img_g = engine.rtm_shot(_prm(c), c["nxSou"], c["nySou"], c["nxRec"], c["nyRec"], c["src"], c["tgt"], c["dd"],
+                            c["dt"], c["ny"], c["nx"], c["nx_w"], c["vp_w"], c["added_space"], 1, c["nt"], c["nt"],
+                            c["nt"])
+    assert np.abs(img_o).max() > 0
+    _assert_same(img_g, img_o, "PSDM_w")
+    F_o, rec_o, F_g, rec_g = _forward_both(engine, oracle, c)
+    _assert_same(F_g, F_o, "Fields")
+    _assert_same(rec_g, rec_o, "Data_synth")
