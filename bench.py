@@ -245,7 +245,10 @@ def run_gpu(args):
     torch.cuda.set_device(dev)
 
     engine = rtm.Engine(local)
-    stream = torch.cuda.current_stream(dev)
+    # One non-default stream for torch ops, NCCL and the engine (handle 0
+    # would mean "the engine's own stream" to psdm_engine_set_stream).
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     engine.set_stream(stream.cuda_stream)
     prm = rtm.Params(dPML=DPML, fs=1, strategy=1)
 

@@ -54,6 +54,10 @@ int fail(int code, const char* fmt, ...) {
 struct psdm_engine {
     int device = 0;
     int num_sms = 148;
+    // Kernels that give up waiting for their copies set this word (host
+    // memory mapped into the device); checked after each synchronisation.
+    volatile int* h_err = nullptr;
+    int* d_err = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;  // own_stream or the caller's
     struct Buf {
@@ -67,6 +71,13 @@ struct psdm_engine {
     bool profiling = false;
     std::vector<cudaEvent_t> events;  // triples (start, forward done, backward done)
     size_t events_used = 0;
+    // Captured step loops, one per pass kind (forward / backward), replayed
+    // while every launch argument is unchanged.
+    struct GraphCache {
+        std::vector<StepArgs> args;
+        cudaGraphExec_t exec = nullptr;
+    } graphs[2];
+    bool use_graphs = true;
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
@@ -76,6 +87,7 @@ struct psdm_engine {
         if (b.bytes < bytes) {
             if (b.ptr) {
                 CUDA_TRY(cudaStreamSynchronize(stream));
+                drop_graphs();  // captured launches may reference this buffer
                 CUDA_TRY(cudaFree(b.ptr));
             }
             b.ptr = nullptr;
@@ -96,10 +108,18 @@ struct psdm_engine {
         return s;
     }
     int trim() {
+        drop_graphs();
         for (auto& kv : bufs)
             if (kv.second.ptr) CUDA_TRY(cudaFree(kv.second.ptr));
         bufs.clear();
         return PSDM_OK;
+    }
+    void drop_graphs() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            g.args.clear();
+        }
     }
     // Profiling marks: 0 = shot start, 1 = forward done, 2 = backward done.
     int record(int which) {
@@ -138,6 +158,7 @@ struct Shot {
     int fast_div = 0;
     int* counters = nullptr;  // two tile counters, alternating per step
     int num_sms = 0;
+    int* err = nullptr;       // device view of the engine's error word
 };
 
 // Injection map (sources or adjoint sources at receivers), last write wins
@@ -213,6 +234,7 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
     TRY(e->get("fB", (size_t)g.dn, &s->fB));
     TRY(e->get("tile_counters", 2, &s->counters));
     s->num_sms = e->num_sms;
+    s->err = e->d_err;
 
     std::vector<float> fA(g.dn), fB(g.dn);
     pml_profiles_f32(kAcc, g.dPML, dt, dd, g.dn, fA.data(), fB.data());
@@ -298,9 +320,9 @@ StepArgs base_args(const Shot& s) {
     a.nyt = s.g.nyt; a.nxt = s.g.nxt; a.ldz = s.g.ldz; a.ny = s.g.ny; a.nx = s.g.nx; a.dn = s.g.dn;
     a.zoff = s.g.zoff; a.ldf = s.g.ldf;
     a.fs = s.fs;
-    plan_tiles(&a);
     a.tile_counter = s.counters;
     a.num_sms = s.num_sms;
+    a.err = s.err;
     a.fs = s.fs;
     a.disk = s.disk;
     a.dt = s.dt;
@@ -329,6 +351,51 @@ void set_buffers(const Shot& s, int it, StepArgs* a) {
     a->side_pm = s.side[c ^ 1];
 }
 
+// Launch the step kernels of one pass.  The launches are captured once into
+// a CUDA graph and the graph is replayed while the argument list is
+// identical (same buffers, geometry, step count and per-step values), which
+// removes the host launch cost per time step.  Falls back to direct launches
+// if the capture is not possible.
+int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args) {
+    if (args.empty()) return PSDM_OK;
+    auto& gc = e->graphs[mode];
+    if (e->use_graphs) {
+        const bool same = gc.exec && gc.args.size() == args.size() &&
+                          std::memcmp(gc.args.data(), args.data(), args.size() * sizeof(StepArgs)) == 0;
+        if (!same) {
+            if (gc.exec) cudaGraphExecDestroy(gc.exec);
+            gc.exec = nullptr;
+            gc.args.clear();
+            cudaStream_t cs = e->own_stream;
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                for (const StepArgs& a : args)
+                    if (launch_step(mode, a, cs) != 0) { ok = false; break; }
+                ok = (cudaStreamEndCapture(cs, &graph) == cudaSuccess) && ok;
+            }
+            if (ok) ok = cudaGraphInstantiate(&gc.exec, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();  // clear a failed capture
+            if (ok) {
+                gc.args = args;
+            } else {
+                gc.exec = nullptr;
+                e->use_graphs = false;
+            }
+        }
+        if (gc.exec) {
+            CUDA_TRY(cudaGraphLaunch(gc.exec, e->stream));
+            return PSDM_OK;
+        }
+    }
+    for (const StepArgs& a : args) {
+        int rc = launch_step(mode, a, e->stream);
+        if (rc) return fail(PSDM_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)rc));
+    }
+    return PSDM_OK;
+}
+
 // Forward pass over k = 2..nt (solver_ac_forward_ram.f90:344-577).
 //   d_S: source trace (nt); d_fields: snapshot slots (nslots of ny*nx) or null;
 //   d_rec: receiver traces (NumRec, nt) or null.
@@ -346,6 +413,7 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
         CUDA_TRY(cudaMemsetAsync(d_rec, 0, (size_t)nrec * nt * sizeof(float), e->stream));
     }
     StepArgs a = base_args(s);
+    plan_tiles(&a, inj.row_slot.data());
     a.row_slot = d_row;
     a.inj_cols = d_cols;
     a.inj_trace = d_S;
@@ -355,6 +423,8 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     a.nrec = d_rec ? nrec : 0;
     a.rec_ld = nt;
     const size_t fstride = g.field_cells();
+    std::vector<StepArgs> steps;
+    steps.reserve(nt > 1 ? nt - 1 : 0);
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
@@ -366,9 +436,9 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
             if (snap > nslots) return fail(PSDM_ERR_ARG, "snapshot slot %d exceeds nt_snap=%d", snap, nslots);
             a.field = d_fields + (size_t)(snap - 1) * fstride;
         }
-        int rc = launch_step(0, a, e->stream);
-        if (rc) return fail(PSDM_ERR_CUDA, "forward step %d: %s", k, cudaGetErrorString((cudaError_t)rc));
+        steps.push_back(a);
     }
+    TRY(launch_steps(e, 0, steps));
     e->launches += nt - 1;
     e->fwd_steps += nt - 1;
     if (d_rec && nrec > 0 && nt >= 2) {
@@ -396,6 +466,7 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
     int *d_row = nullptr, *d_cols = nullptr;
     TRY(upload_inj(e, g, inj, "rec", &d_row, &d_cols));
     StepArgs a = base_args(s);
+    plan_tiles(&a, inj.row_slot.data());
     a.row_slot = d_row;
     a.inj_cols = d_cols;
     a.inj_trace = d_back;
@@ -404,11 +475,14 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
     a.ss = float(store_snap);
     const size_t fstride = g.field_cells();
     int snap = nt_snap;
+    std::vector<StepArgs> steps;
+    steps.reserve(nt > 1 ? nt - 1 : 0);
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
         a.inj_t = reverse ? nt - k + 1 : k - 2;  // Sadj(k-1)
         a.field = nullptr;
+        a.field_w = 1.f;
         if ((k - 1) % store_snap == 0) {
             snap = snap - 1;
             if (d_fields && snap >= slot_lo && snap <= slot_hi && snap >= 1) {
@@ -417,9 +491,9 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
                 if (a.field_w == 0.f) a.field = nullptr;  // zero-padded slot: no contribution
             }
         }
-        int rc = launch_step(1, a, e->stream);
-        if (rc) return fail(PSDM_ERR_CUDA, "backward step %d: %s", k, cudaGetErrorString((cudaError_t)rc));
+        steps.push_back(a);
     }
+    TRY(launch_steps(e, 1, steps));
     e->launches += nt - 1;
     e->bwd_steps += nt - 1;
     return PSDM_OK;
@@ -433,6 +507,10 @@ int check_engine(psdm_engine* e) {
 
 int sync(psdm_engine* e) {
     CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (e->h_err && *e->h_err) {
+        *e->h_err = 0;
+        return fail(PSDM_ERR_CUDA, "a step kernel timed out waiting for its shared-memory copies");
+    }
     return PSDM_OK;
 }
 
@@ -534,6 +612,10 @@ int psdm_engine_create(int32_t device, psdm_engine** out) {
                     err != cudaSuccess ? cudaGetErrorString(err) : "0 devices");
     if (device < 0 || device >= n) return fail(PSDM_ERR_ARG, "device %d out of range (%d devices)", device, n);
     CUDA_TRY(cudaSetDevice(device));
+    {
+        const int rc = prepare_step_kernels();
+        if (rc) return fail(PSDM_ERR_CUDA, "preparing the step kernels: %s", cudaGetErrorString((cudaError_t)rc));
+    }
     psdm_engine* e = new psdm_engine();
     e->device = device;
     cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -543,6 +625,16 @@ int psdm_engine_create(int32_t device, psdm_engine** out) {
         return fail(PSDM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(err));
     }
     e->stream = e->own_stream;
+    void* h = nullptr;
+    err = cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped);
+    if (err == cudaSuccess) err = cudaHostGetDevicePointer((void**)&e->d_err, h, 0);
+    if (err != cudaSuccess) {
+        cudaStreamDestroy(e->own_stream);
+        delete e;
+        return fail(PSDM_ERR_CUDA, "mapped error word: %s", cudaGetErrorString(err));
+    }
+    e->h_err = (volatile int*)h;
+    *e->h_err = 0;
     *out = e;
     return PSDM_OK;
 }
@@ -553,6 +645,7 @@ int psdm_engine_destroy(psdm_engine* e) {
     cudaStreamSynchronize(e->stream);
     int rc = e->trim();
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
+    if (e->h_err) cudaFreeHost((void*)e->h_err);
     cudaStreamDestroy(e->own_stream);
     delete e;
     return rc;
@@ -723,9 +816,19 @@ int psdm_rtm_shot_device(psdm_engine* e, const psdm_params* prm, int32_t NumRec,
                          int32_t nt_prop2, int32_t nt_taper, int32_t taper_option, int32_t N_taper, int32_t N_zeros,
                          float* d_PSDM_w) {
     TRY(check_engine(e));
-    return rtm_shot_core(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_Data_source, d_Data_target, dd, dt, ny, nx,
-                         nx_w, d_Vp_w, added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper,
-                         N_zeros, d_PSDM_w);
+    if (!d_Data_source || !d_Data_target || NumRec < 1 || nt_prop2 < 1 || nt_taper < 1)
+        return fail(PSDM_ERR_ARG, "null argument or empty size");
+    // The traces are copied into engine buffers so that the captured step
+    // loops (whose arguments include the trace pointers) can be replayed.
+    float *d_S = nullptr, *d_tgt = nullptr;
+    TRY(e->get("S", (size_t)nt_prop2, &d_S));
+    TRY(e->get("tgt", (size_t)NumRec * nt_taper, &d_tgt));
+    CUDA_TRY(cudaMemcpyAsync(d_S, d_Data_source, nt_prop2 * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_tgt, d_Data_target, (size_t)NumRec * nt_taper * sizeof(float),
+                             cudaMemcpyDeviceToDevice, e->stream));
+    return rtm_shot_core(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_S, d_tgt, dd, dt, ny, nx, nx_w, d_Vp_w,
+                         added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros,
+                         d_PSDM_w);
 }
 
 int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,

@@ -71,10 +71,9 @@ bool fast_div_exact(float y, float* r, float* lo, float* hi, float* tiny) {
     *r = rr;
     *lo = ldexpf(1.0f, -90);
     *hi = std::min(ldexpf(1.0f, 100), ldexpf(y, 120));
-    // below lo the kernels scale x by 2^64: x*2^64 must stay >= lo, and the
-    // quotient must be normal for the scaling back to be exact
-    *tiny = std::max(ldexpf(1.0f, -154), ldexpf(y, -124));
-    if (!(ldexpf(*tiny, 64) >= *lo)) *tiny = ldexpf(*lo, -64);
+    // below lo the kernels scale x by 2^64 (every nonzero float then lies in
+    // [2^-85, 2^-26], inside [lo, hi]); tiny is kept for reference only
+    *tiny = ldexpf(1.0f, -149);
     if (!(y > 0.f) || !std::isfinite(y) || !std::isfinite(rr)) return false;
     for (uint32_t m = 0; m < (1u << 23); ++m) {
         const uint32_t bits = 0x3f800000u | m;

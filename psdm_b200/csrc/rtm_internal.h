@@ -79,22 +79,28 @@ struct StepArgs {
     float* rec_out;
     int nrec, rec_ld, rec_t;  // rec_t < 0: no gather this step
     // block decomposition (plan_tiles): rect r of type r_type (0 interior
-    // band, 1 C-PML x-strip band, 2 z-strip, 3 corner) covers device rows
+    // band, 1 C-PML x-strip band, 2 z-strip, 3 corner, 4 interior rows with
+    // injection or the free surface) covers device rows
     // [r_zd0, r_zd0+r_h) x columns [r_x0, r_x0+r_w); its tiles are blocks
     // [r_first[r], r_first[r+1]) with r_tz tiles along z.
     int nrect;
-    int r_type[9], r_zd0[9], r_x0[9], r_h[9], r_w[9], r_tz[9], r_first[10];
+    int r_type[16], r_zd0[16], r_x0[16], r_h[16], r_w[16], r_tz[16], r_first[17];
     // persistent scheduling: tile_counter[counter_sel] starts at 0 (cleared
     // by the previous step); num_sms = multiprocessor count of the device
     int* tile_counter;
     int counter_sel;
     int num_sms;
+    int* err;  // set to 1 if a bulk copy did not complete
 };
 
 // Fill the block decomposition of `a` from its grid fields (nyt, nxt, ny,
-// nx, dn, zoff, fs).
-void plan_tiles(StepArgs* a);
+// nx, dn, zoff, fs) and the host copy of the injection row map (ldz
+// entries, or null when nothing is injected).
+void plan_tiles(StepArgs* a, const int* row_slot_host);
 
+// Set kernel attributes (shared memory carve-out, occupancy); call once per
+// device before the first launch.  Returns a cudaError_t value.
+int prepare_step_kernels();
 // Launch one fused forward (mode 0) or backward (mode 1) step on `stream`.
 int launch_step(int mode, const StepArgs& a, void* stream);
 // Receiver gather after the last forward step (Rec(nt-1) and Rec(nt)).

@@ -41,6 +41,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "rtm_internal.h"
 
 namespace psdm {
@@ -78,25 +81,80 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
                         __fmul_rn(__fsub_rn(AT(2), AT(-2)), (c)[2])),                           \
               __fmul_rn(__fsub_rn(AT(3), AT(-3)), (c)[3]))
 
-// x / dt, correctly rounded (see fast_div_exact).  Inputs below div_lo are
-// scaled by 2^64 first (exact), which keeps the result exact as long as the
-// quotient is normal (|x| >= div_tiny); zero, subnormal quotients and huge
-// inputs take the IEEE division.
+// x / dt, correctly rounded (see fast_div_exact).  Inputs below div_lo
+// (which includes every input whose quotient is subnormal) are scaled by 2^64
+// first, which is exact: the scaled quotient q1 is correctly rounded to 24
+// bits, q1 * 2^-64 is exact when the true quotient is normal, and when it is
+// subnormal the only double-rounding case -- q1 * 2^-64 landing exactly half
+// way between two subnormals -- is resolved with the sign of the exact
+// residual x*2^64 - q1*dt.  Zero keeps its sign; only inputs above div_hi, or
+// a dt that failed the host check, use the IEEE division.
 __device__ __forceinline__ float div_dt(const StepArgs& a, float x) {
     const float ax = fabsf(x);
+    if (ax == 0.f) return __fmul_rn(x, a.inv_dt);
+    if (!a.fast_div || ax > a.div_hi) return __fdiv_rn(x, a.dt);
     const bool small = ax < a.div_lo;
     const float xs = small ? __fmul_rn(x, 0x1p64f) : x;
     const float q0 = __fmul_rn(xs, a.inv_dt);
     const float e = __fmaf_rn(-q0, a.dt, xs);
-    float q = __fmaf_rn(e, a.inv_dt, q0);
-    q = small ? __fmul_rn(q, 0x1p-64f) : q;
-    if (ax == 0.f) return __fmul_rn(x, a.inv_dt);  // +-0 keeps its sign
-    if (!a.fast_div || ax > a.div_hi || ax < a.div_tiny) q = __fdiv_rn(x, a.dt);
+    const float q1 = __fmaf_rn(e, a.inv_dt, q0);
+    if (!small) return q1;
+    float q = __fmul_rn(q1, 0x1p-64f);
+    const float diff = __fsub_rn(q1, __fmul_rn(q, 0x1p64f));  // exact
+    if (fabsf(diff) == 0x1p-86f) {                             // half a subnormal step
+        const float e1 = __fmaf_rn(-q1, a.dt, xs);             // sign of (true - q1)
+        if (e1 != 0.f && signbit(e1) == signbit(diff)) q = __fadd_rn(q, copysignf(0x1p-149f, diff));
+    }
     return q;
 }
 
 __device__ __forceinline__ float comp(const float4& v, int r) {
     return r == 0 ? v.x : (r == 1 ? v.y : (r == 2 ? v.z : v.w));
+}
+
+// ---- bulk asynchronous copies (global -> shared) completing on an mbarrier
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the phase `parity` of `bar` for at most ~1 s.  Returns false on
+// timeout (the copies never completed); the caller reports it.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > 1000000000ull) return false;
+    }
 }
 
 // Stage rows [sz0, sz0+4*hq) x columns [sx0, sx0+wx) of p in shared memory
@@ -218,121 +276,186 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
     }
 }
 
-// Interior tile (rect type 0): rows [zd0, zd0+h) are interior rows starting on a
-// 16-byte boundary, columns [x0, x0+w) interior columns, so no stencil
-// centre is clamped and no C-PML term applies.  The free-surface row (the
-// first interior row) and injection rows are handled inline.
+// Interior tile (rect type 0): rows [zd0, zd0+h) are interior rows without
+// injection and without the free-surface row, starting on a 16-byte
+// boundary; columns [x0, x0+w) are interior columns.  No stencil centre is
+// clamped and no C-PML term applies.  p (with its halo), p1 and c2 of the
+// tile are staged in shared memory with bulk asynchronous copies, one per
+// column and array, completing on the block's mbarrier; the backward pass
+// reads the snapshot slot and the image with 16-byte loads one column ahead.
+// Each thread updates 4 rows as two row pairs with the packed FP32x2
+// instructions (per-element rounding of the scalar ones); adds that consume
+// a product stay scalar so that no multiply-add is ever fused.
+// Returns false if the copies did not complete (error reported).
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 neg2(const float2& v) { return make_float2(-v.x, -v.y); }
+// sum_{k=0..3} c[k] * (a(+k) + a(-k)) on a pair, in the reference's order.
+// Tap sums and products are packed; the running sum is accumulated with
+// scalar adds: the compiler may fuse a packed multiply into a following
+// packed add (FFMA2) even when both are written with explicit rounding,
+// which would change the result, and it never fuses scalar RN adds.
+__device__ __forceinline__ float2 sum4(const float2& t0, const float2& t1, const float2& t2, const float2& t3) {
+    return make_float2(__fadd_rn(__fadd_rn(__fadd_rn(t0.x, t1.x), t2.x), t3.x),
+                       __fadd_rn(__fadd_rn(__fadd_rn(t0.y, t1.y), t2.y), t3.y));
+}
+#define D2P(AT, c)                                                        \
+    sum4(__fmul2_rn(__fadd2_rn(AT(0), AT(0)), (c)[0]),                    \
+         __fmul2_rn(__fadd2_rn(AT(1), AT(-1)), (c)[1]),                   \
+         __fmul2_rn(__fadd2_rn(AT(2), AT(-2)), (c)[2]),                   \
+         __fmul2_rn(__fadd2_rn(AT(3), AT(-3)), (c)[3]))
+// a + b with b a fresh product: scalar adds (see above).
+__device__ __forceinline__ float2 add_prod(const float2& a, const float2& b) {
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+
 template <int MODE>
-__device__ __forceinline__ void interior_tile(const StepArgs& a, float* ps, int r, int t) {
-    const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
+__device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int r,
+                                              int t) {
+    const int lane = threadIdx.x, wy = threadIdx.y;
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
     const int z0 = a.r_zd0[r] + tz * TZ, x0 = a.r_x0[r] + tx * TX;
-    const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
+    const int nrows = min(TZ, a.r_zd0[r] + a.r_h[r] - z0);  // a multiple of 4
+    const int ncols = min(TX, a.r_x0[r] + a.r_w[r] - x0);
     const int sz0 = z0 - 4, sx0 = x0 - 3;
-    load_tile(a, ps, sz0, sx0, HQ, WX, tid);
-    __syncthreads();
-
-    const int zd = z0 + 4 * lane;  // first device row of this thread's float4
-    const int xb = x0 + wy * XS;   // first column of this thread
-    if (zd >= zend || xb >= xend) return;
-    const int ncol = min(XS, xend - xb);
     const int dn = a.dn;
+    float* ps = sm;                  // p, (ncols+6) columns of HZ rows
+    float* pms = ps + WX * HZ;       // p1, ncols columns of TZ rows
+    float* c2s = pms + TX * TZ;      // c2
+    if (wy == 0) {
+        const uint32_t prow = (uint32_t)(nrows + 8) * 4u, trow = (uint32_t)nrows * 4u;
+        const uint32_t bytes = (uint32_t)(ncols + 6) * prow + (uint32_t)ncols * trow * 2u;
+        fence_proxy_async();  // the previous tile's shared reads precede these writes
+        if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+        __syncwarp();
+        for (int c = lane; c < ncols + 6; c += 32)
+            bulk_g2s(ps + c * HZ, a.p + (sx0 + c) * a.ldz + sz0, prow, bar);
+        for (int c = lane; c < ncols; c += 32) {
+            const int g = (x0 + c) * a.ldz + z0;
+            bulk_g2s(pms + c * TZ, a.pm + g, trow, bar);
+            bulk_g2s(c2s + c * TZ, a.c2 + g, trow, bar);
+        }
+    }
+    const int q = 4 * lane;        // first tile row of this thread's float4
+    const int c0 = wy * XS;        // first tile column of this thread
+    const bool active = q < nrows && c0 < ncols;
+    const int zd = z0 + q;
     const int z = zd - a.zoff;
-    const bool fsq = a.fs && z == dn;  // first row of this float4 is the free surface
-    int4 rs = make_int4(-1, -1, -1, -1);
-    if (a.row_slot != nullptr) rs = __ldg(reinterpret_cast<const int4*>(a.row_slot + zd));
-    const bool has_inj = rs.x >= 0 || rs.y >= 0 || rs.z >= 0 || rs.w >= 0;
-
+    int fi = (x0 + c0 - dn) * a.ldf + (z - dn);
+    const bool img = MODE == 1 && a.field != nullptr;
+    float4 Fn = make_float4(0.f, 0.f, 0.f, 0.f), In = Fn;
+    if (img && active) {  // first column of the snapshot and image, while the copies land
+        Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi));
+        In = *reinterpret_cast<const float4*>(a.image + fi);
+    }
+    const bool ok = mbar_wait_bounded(bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(a.err, 1);
+        return false;
+    }
+    if (!active) return true;
+    const int ncol = min(XS, ncols - c0);
     const float4* __restrict__ ps4 = reinterpret_cast<const float4*>(ps);
-    const int qr = (zd - sz0) >> 2;
-    const float* __restrict__ c2p = a.c2;
-    float* __restrict__ pmp = a.pm;
+    const int qr = (q + 4) >> 2;   // shared float4 row (halo of 4 rows above)
     float4 win[7];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) win[k] = ps4[(xb - 3 + k - sx0) * HQ + qr];
-    int g = xb * a.ldz + zd;
-    int fi = (xb - dn) * a.ldf + (z - dn);
-    const float* c2 = a.cf2;
-    float4 pmv = *reinterpret_cast<const float4*>(pmp + g);
-    float4 c2v = __ldg(reinterpret_cast<const float4*>(c2p + g));
+    for (int k = 0; k < 6; ++k) win[k] = ps4[(c0 + k) * HQ + qr];
+    float* __restrict__ pmp = a.pm;
+    int g = (x0 + c0) * a.ldz + zd;
+    float2 cc[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cc[k] = make_float2(a.cf2[k], a.cf2[k]);
+    const float2 two = make_float2(2.f, 2.f);
 #pragma unroll
     for (int c = 0; c < XS; ++c) {
         if (c >= ncol) break;
-        const int col = xb + c - sx0;
-        win[6] = ps4[(col + 3) * HQ + qr];
-        const float4 zm = ps4[col * HQ + qr - 1];
-        const float4 zp = ps4[col * HQ + qr + 1];
-        // prefetch the next column's p1 and c2
-        float4 pmn = pmv, c2n = c2v;
-        if (c + 1 < ncol) {
-            pmn = *reinterpret_cast<const float4*>(pmp + g + a.ldz);
-            c2n = __ldg(reinterpret_cast<const float4*>(c2p + g + a.ldz));
+        const int col = c0 + c;    // tile column; shared p column is col + 3
+        win[6] = ps4[(col + 6) * HQ + qr];
+        const float4 zm = ps4[(col + 3) * HQ + qr - 1];
+        const float4 zp = ps4[(col + 3) * HQ + qr + 1];
+        const float4 pmv = *reinterpret_cast<const float4*>(pms + col * TZ + q);
+        const float4 c2v = *reinterpret_cast<const float4*>(c2s + col * TZ + q);
+        float4 Fc = Fn, Ic = In;
+        if (img && c + 1 < ncol) {  // next column of the snapshot and image
+            Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi + a.ldf));
+            In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
         }
-        float src[4] = {0.f, 0.f, 0.f, 0.f};
-        if (has_inj) {
-            const int x = xb + c;
-            const int rsv[4] = {rs.x, rs.y, rs.z, rs.w};
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (rsv[r] >= 0) {
-                    const int j = __ldg(a.inj_cols + rsv[r] * a.nxt + x);
-                    if (j >= 0) src[r] = __ldg(a.inj_trace + (size_t)j * a.inj_ld + a.inj_t);
-                }
-        }
-        const float zv[10] = {zm.y, zm.z, zm.w, win[3].x, win[3].y, win[3].z, win[3].w, zp.x, zp.y, zp.z};
-        float o[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-#define WXR(k) comp(win[3 + (k)], r)
-#define WZR(k) zv[3 + r + (k)]
-            const float d2x = D2(WXR, c2);
-            const float d2y = D2(WZR, c2);
-#undef WXR
-#undef WZR
-            const float base = __fadd_rn(-comp(pmv, r), __fmul_rn(2.f, comp(win[3], r)));
-            float lap = __fadd_rn(d2x, d2y);
-            if (has_inj) lap = __fadd_rn(lap, src[r]);
-            o[r] = __fadd_rn(base, __fmul_rn(comp(c2v, r), lap));
-        }
-        if (fsq) o[0] = 0.f;
-        const float4 out = make_float4(o[0], o[1], o[2], o[3]);
+        const float4& pc = win[3];
+        // z-window rows -3..+6 around the float4: pairs (i, i+1) of
+        // {zm.y, zm.z, zm.w, pc.x, pc.y, pc.z, pc.w, zp.x, zp.y, zp.z}
+        const float2 z01 = make_float2(zm.y, zm.z), z12 = make_float2(zm.z, zm.w);
+        const float2 z23 = make_float2(zm.w, pc.x), z34 = lo2(pc);
+        const float2 z45 = make_float2(pc.y, pc.z), z56 = hi2(pc);
+        const float2 z67 = make_float2(pc.w, zp.x), z78 = lo2(zp);
+        const float2 z89 = make_float2(zp.y, zp.z);
+        // rows 0-1: centre pair z34; rows 2-3: centre pair z56
+#define XA(k) lo2(win[3 + (k)])
+#define XB(k) hi2(win[3 + (k)])
+        const float2 d2xA = D2P(XA, cc);
+        const float2 d2xB = D2P(XB, cc);
+#undef XA
+#undef XB
+        const float2 zA[7] = {z01, z12, z23, z34, z45, z56, z67};
+        const float2 zB[7] = {z23, z34, z45, z56, z67, z78, z89};
+#define ZA(k) zA[3 + (k)]
+#define ZB(k) zB[3 + (k)]
+        const float2 d2yA = D2P(ZA, cc);
+        const float2 d2yB = D2P(ZB, cc);
+#undef ZA
+#undef ZB
+        // -p1 + 2p: 2p is exact, so a fused form would round identically
+        const float2 baseA = __fadd2_rn(neg2(lo2(pmv)), __fmul2_rn(two, lo2(pc)));
+        const float2 baseB = __fadd2_rn(neg2(hi2(pmv)), __fmul2_rn(two, hi2(pc)));
+        const float2 oA = add_prod(baseA, __fmul2_rn(lo2(c2v), __fadd2_rn(d2xA, d2yA)));
+        const float2 oB = add_prod(baseB, __fmul2_rn(hi2(c2v), __fadd2_rn(d2xB, d2yB)));
+        const float4 out = make_float4(oA.x, oA.y, oB.x, oB.y);
         *reinterpret_cast<float4*>(pmp + g) = out;
-        if (a.field != nullptr) {
-            if (MODE == 0) {
-                float4 s;
-                s.x = div_dt(a, __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f));
-                s.y = div_dt(a, __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f));
-                s.z = div_dt(a, __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f));
-                s.w = div_dt(a, __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f));
-                *reinterpret_cast<float4*>(a.field + fi) = s;
-            } else {
-                float4 F = __ldg(reinterpret_cast<const float4*>(a.field + fi));
-                float4 im = *reinterpret_cast<const float4*>(a.image + fi);
-                if (a.field_w != 1.f) {
-                    F.x = __fmul_rn(F.x, a.field_w); F.y = __fmul_rn(F.y, a.field_w);
-                    F.z = __fmul_rn(F.z, a.field_w); F.w = __fmul_rn(F.w, a.field_w);
-                }
-                float4 inc;
-                inc.x = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out.x, pmv.x)), F.x);
-                inc.y = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out.y, pmv.y)), F.y);
-                inc.z = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out.z, pmv.z)), F.z);
-                inc.w = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out.w, pmv.w)), F.w);
-                if (a.ss != 1.f) {
-                    inc.x = __fmul_rn(inc.x, a.ss); inc.y = __fmul_rn(inc.y, a.ss);
-                    inc.z = __fmul_rn(inc.z, a.ss); inc.w = __fmul_rn(inc.w, a.ss);
-                }
-                im.x = __fadd_rn(im.x, inc.x); im.y = __fadd_rn(im.y, inc.y);
-                im.z = __fadd_rn(im.z, inc.z); im.w = __fadd_rn(im.w, inc.w);
-                *reinterpret_cast<float4*>(a.image + fi) = im;
+        if (MODE == 0 && a.field != nullptr) {
+            float4 sv;
+            sv.x = div_dt(a, __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f));
+            sv.y = div_dt(a, __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f));
+            sv.z = div_dt(a, __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f));
+            sv.w = div_dt(a, __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f));
+            *reinterpret_cast<float4*>(a.field + fi) = sv;
+        }
+        if (MODE == 1 && img) {
+            if (a.field_w != 1.f) {
+                Fc.x = __fmul_rn(Fc.x, a.field_w); Fc.y = __fmul_rn(Fc.y, a.field_w);
+                Fc.z = __fmul_rn(Fc.z, a.field_w); Fc.w = __fmul_rn(Fc.w, a.field_w);
             }
+            const float2 half = make_float2(0.5f, 0.5f);
+            float2 iA = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oA, neg2(lo2(pmv)))), lo2(Fc));
+            float2 iB = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oB, neg2(hi2(pmv)))), hi2(Fc));
+            if (a.ss != 1.f) {
+                const float2 ss = make_float2(a.ss, a.ss);
+                iA = __fmul2_rn(iA, ss);
+                iB = __fmul2_rn(iB, ss);
+            }
+            const float2 rA = add_prod(lo2(Ic), iA), rB = add_prod(hi2(Ic), iB);
+            *reinterpret_cast<float4*>(a.image + fi) = make_float4(rA.x, rA.y, rB.x, rB.y);
         }
 #pragma unroll
         for (int k = 0; k < 6; ++k) win[k] = win[k + 1];
-        pmv = pmn;
-        c2v = c2n;
         g += a.ldz;
         fi += a.ldf;
     }
+    return true;
+}
+
+// Interior rows that carry the free surface or injection points (rect type
+// 4): 4 rows x 32 columns per tile, one generic cell per thread.
+template <int MODE>
+__device__ __forceinline__ void rowband_tile(const StepArgs& a, float* ps, int r, int t) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
+    const int z0 = a.r_zd0[r] + tz * 4, x0 = a.r_x0[r] + tx * 32;
+    const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
+    const int sz0 = z0 - 4, sx0 = x0 - 3;  // interior rows and columns: no clamping
+    load_tile(a, ps, sz0, sx0, 3, 38, tid);
+    __syncthreads();
+    const int zd = z0 + (tid & 3), x = x0 + (tid >> 2);
+    if (zd < zend && x < xend) cell_generic<MODE, 12>(a, ps, sz0, sx0, zd, x);
 }
 
 // C-PML x-strip over the interior band rows (rect type 1): rows are interior
@@ -505,10 +628,17 @@ __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
-    __shared__ __align__(16) float ps[WX * HZ];
+constexpr int smem_floats() {
+    return WX * HZ + TX * TZ * 2;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NT) step_kernel(const StepArgs a) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_id;
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid == 0) mbar_init(&bar, 1);
     if (MODE == 0 && a.rec_t >= 0) {
         // Receivers of the previous step: p is that step's p3.
         for (int i = blockIdx.x * NT + tid; i < a.nrec; i += gridDim.x * NT)
@@ -517,6 +647,8 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
     // Persistent blocks take tiles in order (heaviest rect types first) from
     // this step's counter; the other counter is cleared for the next step.
     if (blockIdx.x == 0 && tid == 0) a.tile_counter[a.counter_sel ^ 1] = 0;
+    __syncthreads();
+    uint32_t phase = 0;
     const int total = a.r_first[a.nrect];
     for (;;) {
         if (tid == 0) tile_id = atomicAdd(a.tile_counter + a.counter_sel, 1);
@@ -527,10 +659,13 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
         while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
         const int t = b - a.r_first[r];
         switch (a.r_type[r]) {
-            case 0: interior_tile<MODE>(a, ps, r, t); break;
-            case 1: xband_tile<MODE>(a, ps, r, t); break;
-            case 2: zstrip_tile<MODE>(a, ps, r, t); break;
-            default: generic_tile<MODE>(a, ps, r, t); break;
+            case 0:
+                if (!interior_tile<MODE>(a, sm, &bar, phase, r, t)) return;
+                break;
+            case 1: xband_tile<MODE>(a, sm, r, t); break;
+            case 2: zstrip_tile<MODE>(a, sm, r, t); break;
+            case 4: rowband_tile<MODE>(a, sm, r, t); break;
+            default: generic_tile<MODE>(a, sm, r, t); break;
         }
         __syncthreads();  // shared tile and tile_id are reused
     }
@@ -568,23 +703,47 @@ __global__ void pad_c2_kernel(const float* vp, int ny, int nx, int dn, int nyt, 
 
 }  // namespace
 
-void plan_tiles(StepArgs* a) {
-    // Rects of the padded grid (device rows):
-    //   type 0  interior band  rows [d0, d0+ny4) x interior columns
+void plan_tiles(StepArgs* a, const int* row_slot_host) {
+    // Rects of the padded grid (device rows), heaviest first:
+    //   type 0  interior band rows without injection / free surface
     //   type 1  x-strip band   rows [d0, d0+ny4) x C-PML columns
     //   type 2  z-strips       rows below the band (and above it without a free
     //                          surface) x interior columns
+    //   type 4  interior band rows with injection points or the free surface
     //   type 3  corners        the remaining rows x C-PML columns
     // d0 = first interior row (a multiple of 4), ny4 = ny rounded down to 4.
     const int dn = a->dn, nr = a->zoff + a->nyt;
     const int d0 = dn + a->zoff;
     const int ny4 = a->ny & ~3;
+    const int nq = ny4 / 4;
+    // special float4 rows of the band
+    std::vector<char> special(nq, 0);
+    if (a->fs && nq > 0) special[0] = 1;
+    if (row_slot_host)
+        for (int q = 0; q < nq; ++q)
+            for (int k = 0; k < 4; ++k)
+                if (row_slot_host[d0 + 4 * q + k] >= 0) special[q] = 1;
+    // runs of equal kind; too many runs: one special run spanning them all
+    std::vector<std::pair<int, int>> runs;  // (start quad, kind) boundaries
+    for (int q = 0; q < nq; ++q)
+        if (q == 0 || special[q] != special[q - 1]) runs.push_back({q, special[q]});
+    int nspecial = 0;
+    for (auto& rn : runs) nspecial += rn.second;
+    if (nspecial > 3) {
+        int first = -1, last = -1;
+        for (int q = 0; q < nq; ++q)
+            if (special[q]) { if (first < 0) first = q; last = q; }
+        for (int q = first; q <= last; ++q) special[q] = 1;
+        runs.clear();
+        for (int q = 0; q < nq; ++q)
+            if (q == 0 || special[q] != special[q - 1]) runs.push_back({q, special[q]});
+    }
     int n = 0;
     a->r_first[0] = 0;
     auto add = [&](int type, int zd0, int x0, int h, int w) {
         if (h <= 0 || w <= 0) return;
-        const int tzsz = (type == 0 || type == 1) ? TZ : PTZ;
-        const int txsz = (type == 0) ? TX : PTX;
+        const int tzsz = (type == 0 || type == 1) ? TZ : (type == 4 ? 4 : PTZ);
+        const int txsz = (type == 0 || type == 4) ? TX : PTX;
         a->r_type[n] = type;
         a->r_zd0[n] = zd0; a->r_x0[n] = x0; a->r_h[n] = h; a->r_w[n] = w;
         a->r_tz[n] = (h + tzsz - 1) / tzsz;
@@ -592,39 +751,59 @@ void plan_tiles(StepArgs* a) {
         ++n;
     };
     const int xr = dn + a->nx;  // first right-strip column
-    add(0, d0, dn, ny4, a->nx);
-    add(1, d0, 0, ny4, dn);
-    add(1, d0, xr, ny4, a->nxt - xr);
-    add(2, d0 + ny4, dn, nr - (d0 + ny4), a->nx);
+    for (int kind = 0; kind < 2; ++kind) {
+        if (kind == 1) {  // C-PML x-band after the interior runs
+            add(1, d0, 0, ny4, dn);
+            add(1, d0, xr, ny4, a->nxt - xr);
+            add(2, d0 + ny4, dn, nr - (d0 + ny4), a->nx);
+            if (!a->fs) add(2, 0, dn, d0, a->nx);
+        }
+        for (size_t i = 0; i < runs.size(); ++i) {
+            if (runs[i].second != kind) continue;
+            const int q0 = runs[i].first;
+            const int q1 = (i + 1 < runs.size()) ? runs[i + 1].first : nq;
+            add(kind == 0 ? 0 : 4, d0 + 4 * q0, dn, 4 * (q1 - q0), a->nx);
+        }
+    }
     add(3, d0 + ny4, 0, nr - (d0 + ny4), dn);
     add(3, d0 + ny4, xr, nr - (d0 + ny4), a->nxt - xr);
     if (!a->fs) {  // with a free surface the rows above it are dead
-        add(2, 0, dn, d0, a->nx);
         add(3, 0, 0, d0, dn);
         add(3, 0, xr, d0, a->nxt - xr);
     }
     a->nrect = n;
 }
 
-int step_blocks_per_sm() {
+template <int MODE>
+int blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
-        int n0 = 0, n1 = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, step_kernel<0>, NT, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, step_kernel<1>, NT, 0);
-        nb = max(1, min(n0, n1));
+        const int bytes = smem_floats<MODE>() * (int)sizeof(float);
+        cudaFuncSetAttribute(step_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<MODE>, NT, bytes);
+        nb = n > 0 ? n : 1;
     }
     return nb;
 }
 
-int launch_step(int mode, const StepArgs& a, void* stream) {
-    const dim3 grid(min(a.r_first[a.nrect], a.num_sms * step_blocks_per_sm()));
-    const dim3 block(32, NWARP);
-    if (mode == 0)
-        step_kernel<0><<<grid, block, 0, (cudaStream_t)stream>>>(a);
-    else
-        step_kernel<1><<<grid, block, 0, (cudaStream_t)stream>>>(a);
+template <int MODE>
+int launch_mode(const StepArgs& a, cudaStream_t stream) {
+    const int bytes = smem_floats<MODE>() * (int)sizeof(float);
+    const dim3 grid(min(a.r_first[a.nrect], a.num_sms * blocks_per_sm<MODE>()));
+    step_kernel<MODE><<<grid, dim3(32, NWARP), bytes, stream>>>(a);
     return (int)cudaGetLastError();
+}
+
+int prepare_step_kernels() {
+    // Kernel attributes and occupancy are set up once, outside any stream
+    // capture.
+    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0) ? (int)cudaGetLastError() : 1;
+}
+
+int launch_step(int mode, const StepArgs& a, void* stream) {
+    if (a.r_first[a.nrect] <= 0) return 0;
+    return mode == 0 ? launch_mode<0>(a, (cudaStream_t)stream) : launch_mode<1>(a, (cudaStream_t)stream);
 }
 
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream) {
