@@ -65,6 +65,14 @@ constexpr int PTX = NWARP * PXS;
 constexpr int PHZ = PTZ + 8;
 constexpr int PHQ = PHZ / 4;
 constexpr int PWX = PTX + 6;
+// z-strip tiles: 32 rows x 32 columns (8 columns per thread); row-band
+// tiles: 4 rows x 64 columns (2 cells per thread).  Sized so that, with the
+// interior and x-strip tiles, a step has about as many tiles as resident
+// blocks.
+constexpr int ZXS = 8;
+constexpr int ZTX = NWARP * ZXS;
+constexpr int ZWX = ZTX + 6;
+constexpr int RTX = 64;
 constexpr int NT = 32 * NWARP;  // threads per block
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -444,18 +452,23 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
 }
 
 // Interior rows that carry the free surface or injection points (rect type
-// 4): 4 rows x 32 columns per tile, one generic cell per thread.
+// 4): 4 rows x 64 columns per tile, generic cells, 2 per thread.
 template <int MODE>
 __device__ __forceinline__ void rowband_tile(const StepArgs& a, float* ps, int r, int t) {
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
-    const int z0 = a.r_zd0[r] + tz * 4, x0 = a.r_x0[r] + tx * 32;
+    const int z0 = a.r_zd0[r] + tz * 4, x0 = a.r_x0[r] + tx * RTX;
     const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
     const int sz0 = z0 - 4, sx0 = x0 - 3;  // interior rows and columns: no clamping
-    load_tile(a, ps, sz0, sx0, 3, 38, tid);
+    load_tile(a, ps, sz0, sx0, 3, RTX + 6, tid);
     __syncthreads();
-    const int zd = z0 + (tid & 3), x = x0 + (tid >> 2);
-    if (zd < zend && x < xend) cell_generic<MODE, 12>(a, ps, sz0, sx0, zd, x);
+    const int zd = z0 + (tid & 3);
+    if (zd >= zend) return;
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const int x = x0 + (tid >> 2) + 32 * h;
+        if (x < xend) cell_generic<MODE, 12>(a, ps, sz0, sx0, zd, x);
+    }
 }
 
 // C-PML x-strip over the interior band rows (rect type 1): rows are interior
@@ -545,12 +558,12 @@ template <int MODE>
 __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r, int t) {
     const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
-    const int z0 = a.r_zd0[r] + tz * PTZ, x0 = a.r_x0[r] + tx * PTX;
+    const int z0 = a.r_zd0[r] + tz * PTZ, x0 = a.r_x0[r] + tx * ZTX;
     const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
     const int nr = a.zoff + a.nyt;
     const int sz0 = (min(z0, nr - 4) - 3) & ~3;
     const int sx0 = x0 - 3;  // interior columns: no clamping along x
-    load_tile(a, ps, sz0, sx0, PHQ, PWX, tid);
+    load_tile(a, ps, sz0, sx0, PHQ, ZWX, tid);
     __syncthreads();
     const int zd = z0 + lane;
     if (zd >= zend) return;
@@ -560,8 +573,8 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     const int kz = (z < dn) ? (dn - z) : (z >= dn + a.ny ? z - (dn + a.ny) + 1 : 0);
     if (kz == 0) {
 #pragma unroll 1
-        for (int c = 0; c < PXS; ++c) {
-            const int x = x0 + wy * PXS + c;
+        for (int c = 0; c < ZXS; ++c) {
+            const int x = x0 + wy * ZXS + c;
             if (x >= xend) break;
             cell_generic<MODE, PHZ>(a, ps, sz0, sx0, zd, x);
         }
@@ -575,8 +588,8 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     const float* c1 = a.cf1;
     const float* c2 = a.cf2;
 #pragma unroll 1
-    for (int c = 0; c < PXS; ++c) {
-        const int x = x0 + wy * PXS + c;
+    for (int c = 0; c < ZXS; ++c) {
+        const int x = x0 + wy * ZXS + c;
         if (x >= xend) break;
         const int xl = x - sx0;
         const float* colc = ps + xl * PHZ + zl;
@@ -743,7 +756,7 @@ void plan_tiles(StepArgs* a, const int* row_slot_host) {
     auto add = [&](int type, int zd0, int x0, int h, int w) {
         if (h <= 0 || w <= 0) return;
         const int tzsz = (type == 0 || type == 1) ? TZ : (type == 4 ? 4 : PTZ);
-        const int txsz = (type == 0 || type == 4) ? TX : PTX;
+        const int txsz = type == 0 ? TX : (type == 4 ? RTX : (type == 2 ? ZTX : PTX));
         a->r_type[n] = type;
         a->r_zd0[n] = zd0; a->r_x0[n] = x0; a->r_h[n] = h; a->r_w[n] = w;
         a->r_tz[n] = (h + tzsz - 1) / tzsz;
