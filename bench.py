@@ -232,7 +232,7 @@ def build_inputs(engine, torch, dev, shots, survey, vel_true, vel_mig, prm):
 def run_gpu(args):
     import torch
     import torch.distributed as dist
-    from psdm_b200 import rtm, synth
+    from psdm_b200 import driver, rtm, synth
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,33 +256,24 @@ def run_gpu(args):
     vel_true = synth.config2_model(seed=2)
     vel_mig = synth.smooth_model(vel_true, 100.0, DD)
     n_total = args.warmup + args.steps
-    # round-robin shots: icount = (itimes-1)*numtasks + rank + line_i
-    my_shots = [(i * world + rank) % survey.nshots for i in range(n_total)]
+    # round-robin shots (0-based lines, wrapping over the survey)
+    my_shots = [(driver.shot_of(i + 1, world, rank, 1) - 1) % survey.nshots for i in range(n_total)]
     uniq = sorted(set(my_shots))
     d_src, h_src, items_u = build_inputs(engine, torch, dev, uniq, survey, vel_true, vel_mig, prm)
     by_shot = dict(zip(uniq, items_u))
     items = [by_shot[s] for s in my_shots]
 
-    psdm_sum = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
-    cov_sum = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
+    # window images embedded, summed over ranks once per round and stacked
+    # (calculate_PSDM_RTM.f90:471-497)
+    stack = driver.ImageStack(NY, NX, device=dev)
     d_img = torch.zeros((max(it["nx_w"] for it in items), NY), dtype=torch.float32, device=dev)
-    thread_img = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
-    thread_cov = torch.zeros((NX, NY), dtype=torch.float32, device=dev)
 
     def one_round(it):
         nx_w = it["nx_w"]
         engine.rtm_shot_device(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], d_src.data_ptr(),
                                it["d_obs"].data_ptr(), DD, DT, NY, NX, nx_w, it["d_vp"].data_ptr(), ADDED_SPACE, 1,
                                NT, NT, NT, 0, 1, 0, d_img.data_ptr())
-        thread_img.zero_()
-        thread_cov.zero_()
-        thread_img[it["x_i"] - 1:it["x_f"]] = d_img[:nx_w]
-        thread_cov[it["x_i"] - 1:it["x_f"]] = 1.0
-        if world > 1:
-            dist.all_reduce(thread_img)
-            dist.all_reduce(thread_cov)
-        psdm_sum.add_(thread_img)
-        cov_sum.add_(thread_cov)
+        stack.add_round(d_img, it["x_i"], it["x_f"])
 
     for i in range(args.warmup):
         one_round(items[i])
