@@ -158,6 +158,33 @@ int psdm_model_shot(
     float dt, int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w, float dd_space,
     int32_t nt, float* Data_synth /* (nt, NumRec) out */);
 
+/*
+ * psdm_model_shot without any device allocation; no counterpart in the
+ * reference.  For callers that cannot allocate device memory when they model
+ * a shot: applications whose device memory belongs to their own pool or to
+ * a fixed budget, and plugins that must not touch their host's device heap.
+ * Needs no engine.  The scratch (wavefield, model, C-PML variables, ...)
+ * is one fixed static device array of about 19 MB per GPU that loads this
+ * library, kept until exit.  Limits: rows x columns <= 2^19 cells, where
+ * rows = ny + 2*(dPML+6) plus up to 3 alignment rows, rounded up to a
+ * multiple of 32 (at most 4096) and columns = nx_w + 2*(dPML+6) (at most
+ * 4096); NumRec <= 8192.  Larger shots return PSDM_ERR_ARG with the sizes
+ * in psdm_last_error().
+ * d_Data_source (nt), d_Vp_w (ny, nx_w) and d_Data_synth ((nt, NumRec),
+ * overwritten) are device pointers owned by the caller; nxRec/nyRec are host
+ * arrays.  Work is queued on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) and the call returns when it has finished.  The first call
+ * on a device looks up the scratch's device address and prepares the
+ * kernels; make it before any stream capture begins.  All calls on a device
+ * share the one scratch: calls that overlap on the GPU (other host threads,
+ * or other streams) race and corrupt each other's results.
+ */
+int psdm_model_shot_noalloc(
+    const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+    const int32_t* nxRec, const int32_t* nyRec, const float* d_Data_source, float dd, float dt,
+    int32_t ny, int32_t nx, int32_t nx_w, const float* d_Vp_w, float dd_space, int32_t nt,
+    float* d_Data_synth, void* stream);
+
 /* ---- host helpers: the reference's set-up arithmetic, same FP32 order ---- */
 
 /* finite_difference_coef (src/solver_FD_coeffs.f90:1-73); coef[acc+1]. */

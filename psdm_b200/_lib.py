@@ -22,6 +22,7 @@ EXPORTS = [
     "psdm_engine_reset_stats", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
+    "psdm_model_shot_noalloc",
 ]
 
 
@@ -77,6 +78,7 @@ def lib():
     L.psdm_rtm_shot_device.argtypes = [
         _P, PP, _I, _I, _I, _i32p, _i32p, _P, _P, _F, _F, _I, _I, _I, _P, _F, _I, _I, _I, _I, _I, _I, _I, _P]
     L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
+    L.psdm_model_shot_noalloc.argtypes = [PP, _I, _I, _I, _i32p, _i32p, _P, _F, _F, _I, _I, _I, _P, _F, _I, _P, _P]
     L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
     L.psdm_fd_coef.restype = None
     L.psdm_pml_coeffs.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _P]

@@ -51,6 +51,8 @@ int fail(int code, const char* fmt, ...) {
 
 }  // namespace
 
+void psdm::set_last_error(const char* msg) { g_last_error = msg; }
+
 struct psdm_engine {
     int device = 0;
     int num_sms = 148;

@@ -110,4 +110,7 @@ int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nr
 int launch_pad_c2(const float* vp, int ny, int nx, int dn, int nyt, int nxt, int ldz, int zoff, float dt, float dd,
                   int ram_padding, float* c2, void* stream);
 
+// Record the message that psdm_last_error returns on this thread.
+void set_last_error(const char* msg);
+
 }  // namespace psdm
