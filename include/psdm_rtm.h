@@ -148,6 +148,48 @@ int psdm_rtm_shot_device(
     int32_t nt_taper, int32_t taper_option, int32_t N_taper, int32_t N_zeros, float* d_PSDM_w);
 
 /*
+ * One shot of a batched call.  Geometry in model coordinates as for
+ * psdm_rtm_shot; nxRec/nyRec are host arrays.  Vp_w, Data_target and PSDM_w
+ * are host pointers for psdm_rtm_batch and device pointers for
+ * psdm_rtm_batch_device.
+ */
+typedef struct psdm_shot {
+    int32_t NumRec, nxSou, nySou;
+    const int32_t* nxRec;
+    const int32_t* nyRec;
+    int32_t nx_w;                /* window width (dynamic_window of this geometry) */
+    int32_t nt_prop2, nt_taper;  /* forward steps, data length (>= nt_prop2) */
+    const float* Vp_w;           /* (ny, nx_w) migration model of the window */
+    const float* Data_target;    /* (nt_taper, NumRec), conditioned, not reversed */
+    float* PSDM_w;               /* (ny, nx_w) out, overwritten */
+} psdm_shot;
+
+/*
+ * Many shots through the per-shot block of calculate_PSDM_RTM
+ * (src/calculate_PSDM_RTM.f90:395-466), several at a time: each time step is
+ * one launch that advances every shot in flight (its forward pass, then its
+ * backward pass with the imaging condition), and a finished shot's place is
+ * taken by the next one, so windows and record lengths may differ from shot
+ * to shot.  Up to max_slots shots (at most 16; <= 0 = as many as fit) are in
+ * flight, limited by the free device memory (each holds its FP32 snapshots).
+ * Every PSDM_w equals what psdm_rtm_shot returns for that shot, bit for bit.
+ * Data_source (>= max nt_prop2 samples) is shared by all shots, as in the
+ * reference (one Ricker wavelet per run).  The reference has no batched
+ * interface: it runs one shot per MPI rank at a time.
+ */
+int psdm_rtm_batch(
+    psdm_engine* e, const psdm_params* prm, int32_t nshots, const psdm_shot* shots,
+    const float* Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
+    int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots);
+/* Same with device pointers (Data_source too); returns when all images are written. */
+int psdm_rtm_batch_device(
+    psdm_engine* e, const psdm_params* prm, int32_t nshots, const psdm_shot* shots,
+    const float* d_Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
+    int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots);
+/* Shots in flight at a time in the last batched call. */
+int32_t psdm_engine_batch_slots(const psdm_engine* e);
+
+/*
  * Forward modelling only (the receiver output Rec_point of
  * solver_ac_forward_ram, src/solver_ac_forward_ram.f90:567-577) without
  * storing snapshots: synthetic shot gathers for least-squares or QC.

@@ -22,7 +22,7 @@ EXPORTS = [
     "psdm_engine_reset_stats", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
-    "psdm_model_shot_noalloc",
+    "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
 ]
 
 
@@ -33,6 +33,13 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("fwd_steps", C.c_int64), ("bwd_steps", C.c_int64), ("shots", C.c_int64),
                 ("fwd_ms", C.c_double), ("bwd_ms", C.c_double)]
+
+
+class Shot(C.Structure):
+    """struct psdm_shot (one shot of a batched call)."""
+    _fields_ = [("NumRec", C.c_int32), ("nxSou", C.c_int32), ("nySou", C.c_int32), ("nxRec", C.c_void_p),
+                ("nyRec", C.c_void_p), ("nx_w", C.c_int32), ("nt_prop2", C.c_int32), ("nt_taper", C.c_int32),
+                ("Vp_w", C.c_void_p), ("Data_target", C.c_void_p), ("PSDM_w", C.c_void_p)]
 
 
 class PsdmError(RuntimeError):
@@ -79,6 +86,10 @@ def lib():
         _P, PP, _I, _I, _I, _i32p, _i32p, _P, _P, _F, _F, _I, _I, _I, _P, _F, _I, _I, _I, _I, _I, _I, _I, _P]
     L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
     L.psdm_model_shot_noalloc.argtypes = [PP, _I, _I, _I, _i32p, _i32p, _P, _F, _F, _I, _I, _I, _P, _F, _I, _P, _P]
+    L.psdm_rtm_batch.argtypes = [_P, PP, _I, C.POINTER(Shot), _f32p, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]
+    L.psdm_rtm_batch_device.argtypes = [_P, PP, _I, C.POINTER(Shot), _P, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]
+    L.psdm_engine_batch_slots.argtypes = [_P]
+    L.psdm_engine_batch_slots.restype = _I
     L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
     L.psdm_fd_coef.restype = None
     L.psdm_pml_coeffs.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _P]

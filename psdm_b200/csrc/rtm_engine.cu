@@ -80,6 +80,7 @@ struct psdm_engine {
         cudaGraphExec_t exec = nullptr;
     } graphs[2];
     bool use_graphs = true;
+    int batch_slots = 0;  // slots used by the last batched call
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
@@ -104,6 +105,23 @@ struct psdm_engine {
     int get(const char* name, size_t count, T** out) {
         return get(name, count * sizeof(T), reinterpret_cast<void**>(out));
     }
+    // Grow-only named page-locked host buffer (staging of batched shots).
+    std::map<std::string, Buf> pinned;
+    int get_pinned(const char* name, size_t bytes, void** out) {
+        Buf& b = pinned[name];
+        if (b.bytes < bytes) {
+            if (b.ptr) {
+                CUDA_TRY(cudaStreamSynchronize(stream));
+                CUDA_TRY(cudaFreeHost(b.ptr));
+            }
+            b.ptr = nullptr;
+            b.bytes = 0;
+            CUDA_TRY(cudaMallocHost(&b.ptr, std::max<size_t>(bytes, 256)));
+            b.bytes = std::max<size_t>(bytes, 256);
+        }
+        *out = b.ptr;
+        return PSDM_OK;
+    }
     int64_t total() const {
         int64_t s = 0;
         for (auto& kv : bufs) s += (int64_t)kv.second.bytes;
@@ -114,6 +132,9 @@ struct psdm_engine {
         for (auto& kv : bufs)
             if (kv.second.ptr) CUDA_TRY(cudaFree(kv.second.ptr));
         bufs.clear();
+        for (auto& kv : pinned)
+            if (kv.second.ptr) CUDA_TRY(cudaFreeHost(kv.second.ptr));
+        pinned.clear();
         return PSDM_OK;
     }
     void drop_graphs() {
@@ -208,7 +229,7 @@ int reset_state(psdm_engine* e, Shot* s) {
 // Allocate and initialise the state of a shot from a window model already in
 // device memory (d_vp, (ny, nx) column-major).
 int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd, float dt, const float* d_vp,
-               Shot* s) {
+               Shot* s, const std::string& tag = "") {
     TRY(build_grid(prm, ny, nx, &s->g));
     const Grid& g = s->g;
     // The RAM solvers' padding loops read ctmp(1, j) for j <= dn
@@ -221,20 +242,20 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
     s->fs = prm->fs != 0;
     s->disk = prm->strategy == 2;
     const size_t n = g.cells();
-    TRY(e->get("p0", n, &s->p[0]));
-    TRY(e->get("p1", n, &s->p[1]));
-    TRY(e->get("c2", n, &s->c2));
-    TRY(e->get("phx0", n, &s->phx[0]));
-    TRY(e->get("phx1", n, &s->phx[1]));
-    TRY(e->get("chx", n, &s->chx));
-    TRY(e->get("phz0", n, &s->phz[0]));
-    TRY(e->get("phz1", n, &s->phz[1]));
-    TRY(e->get("chz", n, &s->chz));
-    TRY(e->get("side0", (size_t)g.nxt, &s->side[0]));
-    TRY(e->get("side1", (size_t)g.nxt, &s->side[1]));
-    TRY(e->get("fA", (size_t)g.dn, &s->fA));
-    TRY(e->get("fB", (size_t)g.dn, &s->fB));
-    TRY(e->get("tile_counters", 2, &s->counters));
+    TRY(e->get(("p0" + tag).c_str(), n, &s->p[0]));
+    TRY(e->get(("p1" + tag).c_str(), n, &s->p[1]));
+    TRY(e->get(("c2" + tag).c_str(), n, &s->c2));
+    TRY(e->get(("phx0" + tag).c_str(), n, &s->phx[0]));
+    TRY(e->get(("phx1" + tag).c_str(), n, &s->phx[1]));
+    TRY(e->get(("chx" + tag).c_str(), n, &s->chx));
+    TRY(e->get(("phz0" + tag).c_str(), n, &s->phz[0]));
+    TRY(e->get(("phz1" + tag).c_str(), n, &s->phz[1]));
+    TRY(e->get(("chz" + tag).c_str(), n, &s->chz));
+    TRY(e->get(("side0" + tag).c_str(), (size_t)g.nxt, &s->side[0]));
+    TRY(e->get(("side1" + tag).c_str(), (size_t)g.nxt, &s->side[1]));
+    TRY(e->get(("fA" + tag).c_str(), (size_t)g.dn, &s->fA));
+    TRY(e->get(("fB" + tag).c_str(), (size_t)g.dn, &s->fB));
+    TRY(e->get(("tile_counters" + tag).c_str(), 2, &s->counters));
     s->num_sms = e->num_sms;
     s->err = e->d_err;
 
@@ -398,19 +419,23 @@ int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args) {
     return PSDM_OK;
 }
 
-// Forward pass over k = 2..nt (solver_ac_forward_ram.f90:344-577).
+// Step arguments of a forward pass over k = 2..nt
+// (solver_ac_forward_ram.f90:344-577).
 //   d_S: source trace (nt); d_fields: snapshot slots (nslots of ny*nx) or null;
 //   d_rec: receiver traces (NumRec, nt) or null.
-int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
-                float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec) {
+//   tag: suffix of the engine buffers holding the injection map and the
+//   receiver cells; the per-step arguments are appended to *steps_out.
+int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
+                  float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec, const std::string& tag,
+                  std::vector<StepArgs>* steps_out) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, 1, &zs, &xs, &inj));
     int *d_row = nullptr, *d_cols = nullptr;
-    TRY(upload_inj(e, g, inj, "src", &d_row, &d_cols));
+    TRY(upload_inj(e, g, inj, ("src" + tag).c_str(), &d_row, &d_cols));
     int* d_rec_cell = nullptr;
     if (d_rec && nrec > 0) {
-        TRY(e->get("rec_cell", (size_t)nrec, &d_rec_cell));
+        TRY(e->get(("rec_cell" + tag).c_str(), (size_t)nrec, &d_rec_cell));
         CUDA_TRY(cudaMemcpyAsync(d_rec_cell, h_rec_cell, nrec * sizeof(int), cudaMemcpyHostToDevice, e->stream));
         CUDA_TRY(cudaMemsetAsync(d_rec, 0, (size_t)nrec * nt * sizeof(float), e->stream));
     }
@@ -425,8 +450,8 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     a.nrec = d_rec ? nrec : 0;
     a.rec_ld = nt;
     const size_t fstride = g.field_cells();
-    std::vector<StepArgs> steps;
-    steps.reserve(nt > 1 ? nt - 1 : 0);
+    std::vector<StepArgs>& steps = *steps_out;
+    steps.reserve(steps.size() + (nt > 1 ? nt - 1 : 0));
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
@@ -440,6 +465,17 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
         }
         steps.push_back(a);
     }
+    return PSDM_OK;
+}
+
+// Forward pass over k = 2..nt (solver_ac_forward_ram.f90:344-577).
+//   d_S: source trace (nt); d_fields: snapshot slots (nslots of ny*nx) or null;
+//   d_rec: receiver traces (NumRec, nt) or null.
+int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
+                float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec) {
+    std::vector<StepArgs> steps;
+    TRY(build_forward(e, s, nt, store_snap, d_S, zs, xs, d_fields, nslots, nrec, h_rec_cell, d_rec, "", &steps));
+    const int* d_rec_cell = steps.empty() ? nullptr : steps[0].rec_cell;
     TRY(launch_steps(e, 0, steps));
     e->launches += nt - 1;
     e->fwd_steps += nt - 1;
@@ -452,21 +488,22 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     return PSDM_OK;
 }
 
-// Backward pass over k = 2..nt (solver_ac_backward_ram.f90:329-545).
+// Step arguments of a backward pass over k = 2..nt
+// (solver_ac_backward_ram.f90:329-545); run_backward launches them.
 //   d_back: adjoint traces (nt, NumRec); with reverse = 1 they are read in
 //   reverse time order, which is BackSource(:,j) = Data_target(nt:1:-1, j)
 //   (calculate_PSDM_RTM.f90:448-450) without materialising it.
 //   Snapshots: slot `snap` (1-based) is d_fields + (snap - slot_lo) * ny*nx
 //   when slot_lo <= snap <= slot_hi, and zero otherwise; h_w[snap - 1] is the
 //   taper weight of slot `snap` (size >= nt_snap; null for all ones).
-int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
-                 int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
-                 const float* h_w, float* d_image) {
+int build_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
+                   int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
+                   const float* h_w, float* d_image, const std::string& tag, std::vector<StepArgs>* steps_out) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, nrec, zr, xr, &inj));
     int *d_row = nullptr, *d_cols = nullptr;
-    TRY(upload_inj(e, g, inj, "rec", &d_row, &d_cols));
+    TRY(upload_inj(e, g, inj, ("rec" + tag).c_str(), &d_row, &d_cols));
     StepArgs a = base_args(s);
     plan_tiles(&a, inj.row_slot.data());
     a.row_slot = d_row;
@@ -477,8 +514,8 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
     a.ss = float(store_snap);
     const size_t fstride = g.field_cells();
     int snap = nt_snap;
-    std::vector<StepArgs> steps;
-    steps.reserve(nt > 1 ? nt - 1 : 0);
+    std::vector<StepArgs>& steps = *steps_out;
+    steps.reserve(steps.size() + (nt > 1 ? nt - 1 : 0));
     for (int k = 2; k <= nt; ++k) {
         const int it = k - 2;
         set_buffers(s, it, &a);
@@ -495,6 +532,15 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
         }
         steps.push_back(a);
     }
+    return PSDM_OK;
+}
+
+int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
+                 int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
+                 const float* h_w, float* d_image) {
+    std::vector<StepArgs> steps;
+    TRY(build_backward(e, s, nt, store_snap, nt_snap, d_back, reverse, nrec, zr, xr, d_fields, slot_lo, slot_hi, h_w,
+                       d_image, "", &steps));
     TRY(launch_steps(e, 1, steps));
     e->launches += nt - 1;
     e->bwd_steps += nt - 1;
@@ -596,6 +642,268 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
     CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
                                (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
     return PSDM_OK;
+}
+
+// ---- batched shots ----------------------------------------------------------
+//
+// Several shots ("slots") advance together, one batched launch per time step
+// (batch_step_kernel): each launch takes one step of every active slot, in
+// whichever pass that slot is.  A slot runs its shot's forward pass, then
+// its backward pass with the imaging condition, then takes the next shot of
+// the list, so shots of different window widths and record lengths mix
+// freely.  Every slot owns its wavefield, C-PML state, snapshots and image;
+// the per-step arguments of a shot's two passes are built on the host once,
+// staged through page-locked memory and read by the kernel from HBM.
+
+struct BatchSlot {
+    int shot = -1;       // shot index, -1 = idle
+    int pass = 0;        // 0 forward, 1 backward
+    int k = 0;           // steps of the current pass done
+    int nfwd = 0, nbwd = 0;
+    int tiles[2] = {0, 0};
+    std::string tag;
+    Shot s;
+    StepArgs* d_args = nullptr;  // nfwd forward steps, then nbwd backward steps
+    float* d_imgp = nullptr;     // pitched window image
+    float* d_out = nullptr;      // device variant: caller's image
+    float* h_out = nullptr;      // host variant: caller's image, pending copy-out
+    int out_ny = 0, out_nx = 0;
+    cudaEvent_t staged = nullptr;  // the slot's page-locked staging is free again
+};
+
+struct BatchJob {
+    const psdm_params* prm;
+    const psdm_shot* shots;
+    int nshots;
+    const float* d_S;
+    float dd, dt, added_space;
+    int ny, nx, store_snap, taper_option, N_taper, N_zeros;
+    bool host_io;
+};
+
+int check_batch_shot(const BatchJob& j, int i) {
+    const psdm_shot& sh = j.shots[i];
+    if (sh.NumRec < 1 || !sh.nxRec || !sh.nyRec || !sh.Vp_w || !sh.Data_target || !sh.PSDM_w)
+        return fail(PSDM_ERR_ARG, "shot %d: null argument or NumRec < 1", i);
+    if (sh.nt_prop2 < 2 || sh.nt_taper < sh.nt_prop2)
+        return fail(PSDM_ERR_ARG, "shot %d: need 2 <= nt_prop2 <= nt_taper", i);
+    return PSDM_OK;
+}
+
+// Start shot `i` in slot `sl`: inputs, state, window, per-step arguments.
+int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
+    const psdm_shot& sh = j.shots[i];
+    const int ny = j.ny, nx_w = sh.nx_w;
+    const std::string& tag = sl.tag;
+    const float* d_vp = sh.Vp_w;
+    const float* d_tgt = sh.Data_target;
+    const size_t nvp = (size_t)ny * nx_w, ntgt = (size_t)sh.NumRec * sh.nt_taper;
+    // The slot's page-locked staging is reused only once its previous
+    // copies have completed.
+    CUDA_TRY(cudaEventSynchronize(sl.staged));
+    if (j.host_io) {
+        float *h_vp = nullptr, *h_tgt = nullptr, *dv = nullptr, *dtg = nullptr;
+        TRY(e->get_pinned(("hvp" + tag).c_str(), nvp * sizeof(float), (void**)&h_vp));
+        TRY(e->get_pinned(("htgt" + tag).c_str(), ntgt * sizeof(float), (void**)&h_tgt));
+        std::memcpy(h_vp, sh.Vp_w, nvp * sizeof(float));
+        std::memcpy(h_tgt, sh.Data_target, ntgt * sizeof(float));
+        TRY(e->get(("vp" + tag).c_str(), nvp, &dv));
+        TRY(e->get(("tgt" + tag).c_str(), ntgt, &dtg));
+        CUDA_TRY(cudaMemcpyAsync(dv, h_vp, nvp * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(dtg, h_tgt, ntgt * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        d_vp = dv;
+        d_tgt = dtg;
+    }
+    TRY(setup_shot(e, j.prm, ny, nx_w, j.dd, j.dt, d_vp, &sl.s, tag));
+    WinGeom w;
+    TRY(window_geometry(sl.s.g, sh.NumRec, sh.nxSou, sh.nySou, sh.nxRec, sh.nyRec, j.dd, j.nx, j.added_space, &w));
+    if (w.nx_w_calc != nx_w)
+        return fail(PSDM_ERR_ARG, "shot %d: nx_w=%d does not match the window of its geometry (%d)", i, nx_w,
+                    w.nx_w_calc);
+    const int nt_prop2 = sh.nt_prop2, nt_taper = sh.nt_taper;
+    const int nsnap = (nt_prop2 - 1) / j.store_snap;
+    const size_t fstride = sl.s.g.field_cells();
+    float* d_F = nullptr;
+    if (nsnap > 0) TRY(e->get(("fields" + tag).c_str(), fstride * nsnap, &d_F));
+    TRY(e->get(("imgp" + tag).c_str(), fstride, &sl.d_imgp));
+    // Taper of the snapshot series, as in rtm_shot_core.
+    std::vector<float> wts(std::max(nt_taper, 1), 1.f);
+    if (j.taper_option != 0) {
+        const int i0 = std::max(1, nt_prop2 - j.N_taper + 1);
+        for (int n = 0; n < j.N_taper; ++n)
+            if (i0 + n <= nt_prop2) wts[i0 + n - 1] = taper_weight(n, j.N_taper);
+        if (j.N_zeros > 0)
+            for (int t = nt_prop2; t < nt_taper; ++t) wts[t] = 0.f;
+    }
+    std::vector<StepArgs> steps;
+    TRY(build_forward(e, sl.s, nt_prop2, j.store_snap, j.d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr, tag,
+                      &steps));
+    sl.nfwd = (int)steps.size();
+    TRY(build_backward(e, sl.s, nt_taper, j.store_snap, nt_taper, d_tgt, 1, sh.NumRec, w.zr.data(), w.xr.data(),
+                       d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps));
+    sl.nbwd = (int)steps.size() - sl.nfwd;
+    sl.tiles[0] = sl.nfwd > 0 ? steps[0].r_first[steps[0].nrect] : 0;
+    sl.tiles[1] = sl.nbwd > 0 ? steps[sl.nfwd].r_first[steps[sl.nfwd].nrect] : 0;
+    const size_t abytes = steps.size() * sizeof(StepArgs);
+    StepArgs* h_args = nullptr;
+    TRY(e->get_pinned(("hargs" + tag).c_str(), abytes, (void**)&h_args));
+    std::memcpy(h_args, steps.data(), abytes);
+    TRY(e->get(("args" + tag).c_str(), abytes, (void**)&sl.d_args));
+    CUDA_TRY(cudaMemcpyAsync(sl.d_args, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaEventRecord(sl.staged, e->stream));
+    CUDA_TRY(cudaMemsetAsync(sl.d_imgp, 0, fstride * sizeof(float), e->stream));
+    sl.shot = i;
+    sl.pass = sl.nfwd > 0 ? 0 : 1;
+    sl.k = 0;
+    sl.out_ny = ny;
+    sl.out_nx = nx_w;
+    sl.d_out = j.host_io ? nullptr : sh.PSDM_w;
+    sl.h_out = nullptr;
+    return PSDM_OK;
+}
+
+// Host variant: copy a finished image out of the slot's page-locked buffer.
+int batch_flush(psdm_engine* e, BatchSlot& sl) {
+    if (!sl.h_out) return PSDM_OK;
+    CUDA_TRY(cudaEventSynchronize(sl.staged));
+    void* h_img = nullptr;
+    const size_t bytes = (size_t)sl.out_ny * sl.out_nx * sizeof(float);
+    TRY(e->get_pinned(("himg" + sl.tag).c_str(), bytes, &h_img));
+    std::memcpy(sl.h_out, h_img, bytes);
+    sl.h_out = nullptr;
+    return PSDM_OK;
+}
+
+// The slot's shot is done: hand its image to the caller.
+int batch_finish(psdm_engine* e, const BatchJob& j, BatchSlot& sl) {
+    const size_t ld = (size_t)sl.s.g.ldf * sizeof(float), row = (size_t)sl.out_ny * sizeof(float);
+    if (j.host_io) {
+        // D2H into page-locked memory; batch_flush copies it out once done.
+        float* h_img = nullptr;
+        CUDA_TRY(cudaEventSynchronize(sl.staged));
+        TRY(e->get_pinned(("himg" + sl.tag).c_str(), row * sl.out_nx, (void**)&h_img));
+        CUDA_TRY(cudaMemcpy2DAsync(h_img, row, sl.d_imgp, ld, row, sl.out_nx, cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaEventRecord(sl.staged, e->stream));
+        sl.h_out = j.shots[sl.shot].PSDM_w;
+    } else {
+        CUDA_TRY(cudaMemcpy2DAsync(sl.d_out, row, sl.d_imgp, ld, row, sl.out_nx, cudaMemcpyDeviceToDevice,
+                                   e->stream));
+    }
+    return PSDM_OK;
+}
+
+int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
+    if (j.nshots <= 0) return PSDM_OK;
+    for (int i = 0; i < j.nshots; ++i) TRY(check_batch_shot(j, i));
+    // Slots: as many as asked for, at most kMaxSlots, and as many as fit in
+    // the free device memory with every slot sized for the largest shot.
+    size_t per_slot = 0;
+    for (int i = 0; i < j.nshots; ++i) {
+        Grid g;
+        TRY(build_grid(j.prm, j.ny, j.shots[i].nx_w, &g));
+        const size_t nsnap = (size_t)(j.shots[i].nt_prop2 - 1) / j.store_snap;
+        const size_t steps = (size_t)j.shots[i].nt_prop2 + j.shots[i].nt_taper;
+        size_t b = 9 * g.cells() * sizeof(float) + (nsnap + 1) * g.field_cells() * sizeof(float) +
+                   steps * sizeof(StepArgs);
+        if (j.host_io) b += ((size_t)j.ny * j.shots[i].nx_w + (size_t)j.shots[i].NumRec * j.shots[i].nt_taper) *
+                            sizeof(float);
+        per_slot = std::max(per_slot, b);
+    }
+    const size_t reserve = (size_t)1 << 30;
+    auto slots_that_fit = [&](int* fit, size_t* free_b) -> int {
+        size_t total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(free_b, &total_b));
+        *fit = *free_b > reserve ? (int)std::min<size_t>((*free_b - reserve) / std::max<size_t>(per_slot, 1),
+                                                         (size_t)kMaxSlots)
+                                 : 0;
+        return PSDM_OK;
+    };
+    int nslots = std::min(std::min(max_slots > 0 ? max_slots : kMaxSlots, kMaxSlots), j.nshots);
+    int fit = 0;
+    size_t free_b = 0;
+    TRY(slots_that_fit(&fit, &free_b));
+    if (fit < nslots && e->total() > 0) {
+        // The engine's cached buffers (earlier shots or batches) may hold the
+        // memory: release them and count again.
+        CUDA_TRY(cudaStreamSynchronize(e->stream));
+        TRY(e->trim());
+        TRY(slots_that_fit(&fit, &free_b));
+    }
+    nslots = std::min(nslots, fit);
+    if (nslots < 1)
+        return fail(PSDM_ERR_NOMEM, "one batch slot needs %.1f GB of device memory, %.1f GB are free",
+                    per_slot / 1e9, free_b / 1e9);
+    e->batch_slots = nslots;
+    int* counters = nullptr;
+    TRY(e->get("batch_counters", 2, &counters));
+    CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(int), e->stream));
+    std::vector<BatchSlot> slots(nslots);
+    int rc = PSDM_OK;
+    for (int k = 0; k < nslots; ++k) {
+        slots[k].tag = "_b" + std::to_string(k);
+        if (cudaEventCreateWithFlags(&slots[k].staged, cudaEventDisableTiming) != cudaSuccess) {
+            rc = fail(PSDM_ERR_CUDA, "cudaEventCreate failed");
+            break;
+        }
+    }
+    int next = 0;
+    for (int k = 0; rc == PSDM_OK && k < nslots && next < j.nshots; ++k) rc = batch_start(e, j, slots[k], next++);
+    int sel = 0;
+    while (rc == PSDM_OK) {
+        BatchParams bp;
+        std::memset(&bp, 0, sizeof(bp));
+        int n = 0;
+        for (BatchSlot& sl : slots) {
+            if (sl.shot < 0) continue;
+            bp.mode[n] = sl.pass;
+            bp.args[n] = sl.d_args + (sl.pass == 0 ? sl.k : sl.nfwd + sl.k);
+            bp.first[n + 1] = bp.first[n] + sl.tiles[sl.pass];
+            ++n;
+        }
+        if (n == 0) break;
+        bp.nslots = n;
+        bp.counter = counters;
+        bp.counter_sel = sel;
+        sel ^= 1;
+        const int lr = launch_batch_step(bp, e->num_sms, e->stream);
+        if (lr) {
+            rc = fail(PSDM_ERR_CUDA, "batched step launch: %s", cudaGetErrorString((cudaError_t)lr));
+            break;
+        }
+        e->launches += 1;
+        for (BatchSlot& sl : slots) {
+            if (sl.shot < 0) continue;
+            sl.k += 1;
+            if (sl.pass == 0) {
+                e->fwd_steps += 1;
+                if (sl.k < sl.nfwd) continue;
+                // Second propagator call on the same model: fresh wavefield.
+                rc = reset_state(e, &sl.s);
+                sl.pass = 1;
+                sl.k = 0;
+                if (rc != PSDM_OK) break;
+                if (sl.nbwd > 0) continue;
+            } else {
+                e->bwd_steps += 1;
+                if (sl.k < sl.nbwd) continue;
+            }
+            rc = batch_finish(e, j, sl);
+            sl.shot = -1;
+            if (rc == PSDM_OK && next < j.nshots) {
+                rc = batch_flush(e, sl);
+                if (rc == PSDM_OK) rc = batch_start(e, j, sl, next++);
+            }
+            if (rc != PSDM_OK) break;
+        }
+    }
+    for (BatchSlot& sl : slots) {
+        if (rc == PSDM_OK) rc = batch_flush(e, sl);
+        if (sl.staged) {
+            cudaEventSynchronize(sl.staged);
+            cudaEventDestroy(sl.staged);
+        }
+    }
+    return rc;
 }
 
 }  // namespace
@@ -832,6 +1140,43 @@ int psdm_rtm_shot_device(psdm_engine* e, const psdm_params* prm, int32_t NumRec,
                          added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros,
                          d_PSDM_w);
 }
+
+int psdm_rtm_batch(psdm_engine* e, const psdm_params* prm, int32_t nshots, const psdm_shot* shots,
+                   const float* Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
+                   int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots) {
+    TRY(check_engine(e));
+    TRY(check_params(prm));
+    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (nshots < 0 || (nshots > 0 && (!shots || !Data_source))) return fail(PSDM_ERR_ARG, "null argument");
+    if (store_snap < 1) return fail(PSDM_ERR_ARG, "store_snap must be >= 1");
+    if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
+    int ntmax = 0;
+    for (int i = 0; i < nshots; ++i) ntmax = std::max(ntmax, shots[i].nt_prop2);
+    float* d_S = nullptr;
+    TRY(e->get("S", (size_t)std::max(ntmax, 1), &d_S));
+    CUDA_TRY(cudaMemcpyAsync(d_S, Data_source, (size_t)ntmax * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    BatchJob j{prm, shots, nshots, d_S, dd, dt, added_space, ny, nx, store_snap, taper_option, N_taper, N_zeros, true};
+    TRY(run_batch(e, j, max_slots));
+    return sync(e);
+}
+
+int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots, const psdm_shot* shots,
+                          const float* d_Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
+                          int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros,
+                          int32_t max_slots) {
+    TRY(check_engine(e));
+    TRY(check_params(prm));
+    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (nshots < 0 || (nshots > 0 && (!shots || !d_Data_source))) return fail(PSDM_ERR_ARG, "null argument");
+    if (store_snap < 1) return fail(PSDM_ERR_ARG, "store_snap must be >= 1");
+    if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
+    BatchJob j{prm, shots, nshots, d_Data_source, dd, dt, added_space, ny, nx, store_snap, taper_option, N_taper,
+               N_zeros, false};
+    TRY(run_batch(e, j, max_slots));
+    return sync(e);
+}
+
+int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
 
 int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
                     const int32_t* nxRec, const int32_t* nyRec, const float* Data_source, float dd, float dt,

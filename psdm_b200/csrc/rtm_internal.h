@@ -93,6 +93,21 @@ struct StepArgs {
     int* err;  // set to 1 if a bulk copy did not complete
 };
 
+// One launch advancing several shots ("slots") by one time step each:
+// slot s runs pass mode[s] (0 forward, 1 backward) with the step arguments
+// at args[s] (device memory); its tiles are [first[s], first[s+1]) of the
+// launch's work list, first[s+1] - first[s] = that step's r_first[nrect].
+// counter[counter_sel] starts at 0; the launch clears the other one.
+constexpr int kMaxSlots = 16;
+struct BatchParams {
+    int nslots;
+    int counter_sel;
+    int* counter;
+    int mode[kMaxSlots];
+    int first[kMaxSlots + 1];
+    const StepArgs* args[kMaxSlots];
+};
+
 // Fill the block decomposition of `a` from its grid fields (nyt, nxt, ny,
 // nx, dn, zoff, fs) and the host copy of the injection row map (ldz
 // entries, or null when nothing is injected).
@@ -103,6 +118,8 @@ void plan_tiles(StepArgs* a, const int* row_slot_host);
 int prepare_step_kernels();
 // Launch one fused forward (mode 0) or backward (mode 1) step on `stream`.
 int launch_step(int mode, const StepArgs& a, void* stream);
+// Launch one batched step (batch_step_kernel) on `stream`.
+int launch_batch_step(const BatchParams& bp, int num_sms, void* stream);
 // Receiver gather after the last forward step (Rec(nt-1) and Rec(nt)).
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream);
 // Padded c2 = c^2 dt^2 / d^2 from the window model (edge replication;

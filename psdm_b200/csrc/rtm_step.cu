@@ -684,6 +684,77 @@ __global__ void __launch_bounds__(NT) step_kernel(const StepArgs a) {
     }
 }
 
+// One tile (block-local index b of the step described by `a`).  Returns
+// false if its bulk copies did not complete.
+template <int MODE>
+__device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int b) {
+    int r = 0;
+    while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
+    const int t = b - a.r_first[r];
+    switch (a.r_type[r]) {
+        case 0: return interior_tile<MODE>(a, sm, bar, phase, r, t);
+        case 1: xband_tile<MODE>(a, sm, r, t); return true;
+        case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
+        case 4: rowband_tile<MODE>(a, sm, r, t); return true;
+        default: generic_tile<MODE>(a, sm, r, t); return true;
+    }
+}
+
+// One time step of several shots (slots) in one launch.  The tiles of all
+// slots form one work list, slot s owning tiles [first[s], first[s+1]);
+// persistent blocks take tiles from one counter, so a block moves on to the
+// next slot's tiles while others are still waiting for their copies, and a
+// step of many shots fills the GPU in several waves.  Each slot's step
+// arguments live in device memory; a block copies them into shared memory
+// when it switches slot.  Slots may be in different passes (mode 0 / 1).
+__global__ void __launch_bounds__(NT) batch_step_kernel(const BatchParams bp) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int tile_id;
+    __shared__ __align__(16) StepArgs sa;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid == 0) mbar_init(&bar, 1);
+    // Deferred receiver gathers of the forward slots (p = previous step's p3).
+    for (int s = 0; s < bp.nslots; ++s) {
+        if (bp.mode[s] != 0) continue;
+        const StepArgs* g = bp.args[s];
+        const int rec_t = g->rec_t, nrec = g->nrec;
+        if (rec_t < 0 || nrec <= 0) continue;
+        const float* p = g->p;
+        const int* cell = g->rec_cell;
+        float* out = g->rec_out;
+        const int ld = g->rec_ld;
+        for (int i = blockIdx.x * NT + tid; i < nrec; i += gridDim.x * NT)
+            out[(size_t)i * ld + rec_t] = p[cell[i]];
+    }
+    if (blockIdx.x == 0 && tid == 0) bp.counter[bp.counter_sel ^ 1] = 0;
+    __syncthreads();
+    uint32_t phase = 0;
+    int cur = -1;
+    const int total = bp.first[bp.nslots];
+    constexpr int kWords = (int)(sizeof(StepArgs) / sizeof(long long));
+    static_assert(sizeof(StepArgs) % sizeof(long long) == 0, "StepArgs is copied in 8-byte words");
+    for (;;) {
+        if (tid == 0) tile_id = atomicAdd(bp.counter + bp.counter_sel, 1);
+        __syncthreads();
+        const int b = tile_id;
+        if (b >= total) return;
+        int s = 0;
+        while (s + 1 < bp.nslots && b >= bp.first[s + 1]) ++s;
+        if (s != cur) {  // every thread takes the same branch
+            const long long* src = reinterpret_cast<const long long*>(bp.args[s]);
+            long long* dst = reinterpret_cast<long long*>(&sa);
+            for (int i = tid; i < kWords; i += NT) dst[i] = src[i];
+            __syncthreads();
+            cur = s;
+        }
+        const int lb = b - bp.first[s];
+        const bool ok = bp.mode[s] == 0 ? run_tile<0>(sa, sm, &bar, phase, lb) : run_tile<1>(sa, sm, &bar, phase, lb);
+        if (!ok) return;
+        __syncthreads();  // shared tile, tile_id and (next switch) sa are reused
+    }
+}
+
 __global__ void rec_final_kernel(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrec) return;
@@ -800,6 +871,18 @@ int blocks_per_sm() {
     return nb;
 }
 
+int batch_blocks_per_sm() {
+    static int nb = 0;
+    if (nb == 0) {
+        const int bytes = smem_floats<0>() * (int)sizeof(float);
+        cudaFuncSetAttribute(batch_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_step_kernel, NT, bytes);
+        nb = n > 0 ? n : 1;
+    }
+    return nb;
+}
+
 template <int MODE>
 int launch_mode(const StepArgs& a, cudaStream_t stream) {
     const int bytes = smem_floats<MODE>() * (int)sizeof(float);
@@ -811,12 +894,22 @@ int launch_mode(const StepArgs& a, cudaStream_t stream) {
 int prepare_step_kernels() {
     // Kernel attributes and occupancy are set up once, outside any stream
     // capture.
-    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0) ? (int)cudaGetLastError() : 1;
+    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && batch_blocks_per_sm() > 0) ? (int)cudaGetLastError()
+                                                                                            : 1;
 }
 
 int launch_step(int mode, const StepArgs& a, void* stream) {
     if (a.r_first[a.nrect] <= 0) return 0;
     return mode == 0 ? launch_mode<0>(a, (cudaStream_t)stream) : launch_mode<1>(a, (cudaStream_t)stream);
+}
+
+int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
+    const int total = bp.first[bp.nslots];
+    if (bp.nslots <= 0 || total <= 0) return 0;
+    const int bytes = smem_floats<0>() * (int)sizeof(float);
+    const dim3 grid(min(total, num_sms * batch_blocks_per_sm()));
+    batch_step_kernel<<<grid, dim3(32, NWARP), bytes, (cudaStream_t)stream>>>(bp);
+    return (int)cudaGetLastError();
 }
 
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream) {

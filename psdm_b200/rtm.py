@@ -154,6 +154,48 @@ class Engine:
             d_Data_target, dd, dt, ny, nx, nx_w, d_Vp_w, added_space, store_snap, nt_snap, nt_prop2, nt_taper,
             taper_option, N_taper, N_zeros, d_PSDM_w))
 
+    def rtm_batch(self, prm: Params, shots, Data_source, dd, dt, ny, nx, added_space, store_snap=1,
+                  taper_option=0, N_taper=1, N_zeros=0, max_slots=0):
+        """psdm_rtm_batch over host arrays.  `shots` is a list of dicts with keys
+        nxSou, nySou, nxRec, nyRec, nx_w, nt_prop2, nt_taper, Vp_w (nx_w, ny),
+        Data_target (NumRec, nt_taper); returns the window images (nx_w, ny)."""
+        keep, descs, outs = [], [], []
+        for sh in shots:
+            nxr, nyr = _i32(sh["nxRec"]), _i32(sh["nyRec"])
+            vp, tgt = _f32(sh["Vp_w"]), _f32(sh["Data_target"])
+            nx_w = int(sh["nx_w"])
+            assert vp.shape == (nx_w, ny) and tgt.size == nxr.size * int(sh["nt_taper"])
+            out = np.zeros((nx_w, ny), dtype=np.float32)
+            keep += [nxr, nyr, vp, tgt]
+            outs.append(out)
+            descs.append(L.Shot(nxr.size, int(sh["nxSou"]), int(sh["nySou"]), nxr.ctypes.data, nyr.ctypes.data,
+                                nx_w, int(sh["nt_prop2"]), int(sh["nt_taper"]), vp.ctypes.data, tgt.ctypes.data,
+                                out.ctypes.data))
+        arr = (L.Shot * max(len(descs), 1))(*descs)
+        L.check(L.lib().psdm_rtm_batch(self._h, C.byref(prm.c()), len(descs), arr, _f32(Data_source).reshape(-1),
+                                       dd, dt, ny, nx, added_space, store_snap, taper_option, N_taper, N_zeros,
+                                       max_slots))
+        return outs
+
+    def rtm_batch_device(self, prm: Params, shots, d_Data_source: int, dd, dt, ny, nx, added_space, store_snap=1,
+                         taper_option=0, N_taper=1, N_zeros=0, max_slots=0):
+        """psdm_rtm_batch_device: each shot dict carries device pointers (ints)
+        d_Vp_w, d_Data_target, d_PSDM_w besides its geometry."""
+        keep, descs = [], []
+        for sh in shots:
+            nxr, nyr = _i32(sh["nxRec"]), _i32(sh["nyRec"])
+            keep += [nxr, nyr]
+            descs.append(L.Shot(nxr.size, int(sh["nxSou"]), int(sh["nySou"]), nxr.ctypes.data, nyr.ctypes.data,
+                                int(sh["nx_w"]), int(sh["nt_prop2"]), int(sh["nt_taper"]), int(sh["d_Vp_w"]),
+                                int(sh["d_Data_target"]), int(sh["d_PSDM_w"])))
+        arr = (L.Shot * max(len(descs), 1))(*descs)
+        L.check(L.lib().psdm_rtm_batch_device(self._h, C.byref(prm.c()), len(descs), arr, int(d_Data_source), dd,
+                                              dt, ny, nx, added_space, store_snap, taper_option, N_taper, N_zeros,
+                                              max_slots))
+
+    def batch_slots(self) -> int:
+        return int(L.lib().psdm_engine_batch_slots(self._h))
+
     def model_shot(self, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, dd, dt, ny, nx, nx_w,
                    Vp_w, dd_space, nt):
         """Forward modelling (Rec_point of solver_ac_forward_ram); returns (NumRec, nt)."""
