@@ -78,6 +78,21 @@ def algorithmic_bytes(ny, nx_w, dpml, fs=1):
     return base + 4 * g["n_int"], base + 12 * g["n_int"], g
 
 
+def profiled_traffic(which: str):
+    """DRAM bytes (read + write) per launch of the step kernel from the ncu
+    capture summarised in profiles/ (a `traffic_bytes_per_launch:` line), or
+    None if there is none."""
+    import re
+    p = os.path.join(ROOT, "profiles", "step_kernel_config2_ncu_full.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        m = re.search(r"traffic_bytes_per_launch:\s*fwd=(\d+)\s+bwd=(\d+)", f.read())
+    if not m:
+        return None
+    return int(m.group(1) if which == "fwd" else m.group(2))
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
@@ -311,11 +326,7 @@ def run_gpu(args):
     bytes_dom = bwd_b if dom == "bwd" else fwd_b
     us_dom = bwd_us if dom == "bwd" else fwd_us
     achieved = bytes_dom / (us_dom * 1e-6) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get("step_kernel_bwd" if dom == "bwd" else "step_kernel_fwd")
+    traffic = profiled_traffic(dom)
 
     # end-to-end through the C ABI with pinned host buffers
     e2e = None

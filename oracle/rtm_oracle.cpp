@@ -35,6 +35,11 @@
 //   src/calculate_PSDM_RTM.f90:395-466       per-shot forward/taper/backward
 //   src/auxiliar_PSDM.f90:1-20               normalize_psdm
 //
+// The mixed-precision form (MixedOpts, rtm_shot_mixed) has no reference
+// counterpart: it restates the engine's FP16/BF16-snapshot form so that the
+// float build checks the engine bit for bit and the double build is its FP64
+// oracle.
+//
 // Build: oracle/Makefile (g++ -O3 -ffp-contract=off, no -ffast-math).
 
 #include <cmath>
@@ -301,6 +306,67 @@ void scatter(Arr2<T>& p3, const Strip<T>& s, const std::vector<int>& vy, const s
         for (int j = 1; j <= s.ny; ++j) p3(vy[j - 1], vx[i - 1]) = s.p3(j, i);
 }
 
+// ---- mixed-precision form (no reference counterpart) ------------------------
+//
+// Options of the engine's mixed-precision form, restated here so that the
+// float build emulates the engine bit for bit and the double build is its
+// FP64 oracle:
+//   pair_mode 1: snapshots every store_snap forward steps (slot m at forward
+//     step k = store_snap*m + 1, as the reference stores them) and imaging at
+//     the backward steps paired with them in time, k_b = nt + 1 - store_snap*m
+//     (for store_snap = 1 this is the reference's pairing);
+//   q16: snapshots rounded to binary16 (1) or bfloat16 (2) after scaling by a
+//     power of two 2^k chosen from the snapshot's largest magnitude A so that
+//     A*2^k lies in [2^14, 2^15); read back as float(h) * 2^-k;
+//   kahan: the image is summed with compensated (Kahan) summation.
+struct MixedOpts {
+    int pair_mode = 0;
+    int q16 = 0;
+    int kahan = 0;
+};
+
+// x rounded to the nearest binary16 (mant = 10, emin = -14) or bfloat16
+// (mant = 7, emin = -126) value, ties to even, returned as a float; |x| is
+// far below either format's overflow threshold here.
+inline float round_to_format(float x, int mant, int emin) {
+    const double a = std::fabs((double)x);
+    if (a == 0.0) return x;
+    int e = 0;
+    std::frexp(a, &e);  // a = f * 2^e, f in [0.5, 1)
+    const int E = std::max(e - 1, emin);
+    const double ulp = std::ldexp(1.0, E - mant);
+    const double q = std::nearbyint(a / ulp) * ulp;  // a / ulp is exact
+    return (float)std::copysign(q, (double)x);
+}
+
+// Scale exponent k for a snapshot whose largest magnitude is amax.
+inline int snapshot_scale_exp(float amax) {
+    if (!(amax > 0.f)) return 0;
+    uint32_t b;
+    std::memcpy(&b, &amax, 4);
+    const int E = (int)((b >> 23) & 0xffu) - 127;  // floor(log2 amax); -127 for subnormals
+    return std::min(126, std::max(-126, 14 - E));
+}
+
+inline float pow2f(int k) {
+    uint32_t b = (uint32_t)(k + 127) << 23;  // k in [-126, 127]
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+// Quantize one snapshot in place (float build only).
+template <class T>
+void quantize_snapshot(T* F, size_t n, int q16) {
+    if (q16 == 0 || sizeof(T) != sizeof(float)) return;
+    float amax = 0.f;
+    for (size_t i = 0; i < n; ++i) amax = std::max(amax, (float)std::fabs((float)F[i]));
+    const int k = snapshot_scale_exp(amax);
+    const float sc = pow2f(k), isc = pow2f(-k);
+    const int mant = q16 == 1 ? 10 : 7, emin = q16 == 1 ? -14 : -126;
+    for (size_t i = 0; i < n; ++i) F[i] = (T)(round_to_format((float)F[i] * sc, mant, emin) * isc);
+}
+
 // The propagator, src/solver_ac_forward_ram.f90:4-637 (iprop = 1) and
 // src/solver_ac_backward_ram.f90:4-598 (iprop = 2).  disk_mode = 1 follows
 // the disk variants' order (solver_ac_forward_disk.f90:506-517), in which the
@@ -316,7 +382,9 @@ void solver_ac(int iprop, int disk_mode, int dPML, int fs, int NumRec,
                const T* S /*forward: S(nt); backward: Sadj(nt,NumRec)*/,
                T dmodel, T dt, int ny, int nx, const T* ctmp_in,
                int store_snap, int nt_snap, int nt, T* Fields, T* out /*Rec or kernel*/,
-               T* p_dump = nullptr /*(nyt, nxt) padded p after the last step, optional*/) {
+               T* p_dump = nullptr /*(nyt, nxt) padded p after the last step, optional*/,
+               const MixedOpts* mo = nullptr /*mixed-precision form; null = the reference*/,
+               const T* mixed_weights = nullptr /*mixed form: weight of slot m at [m-1], or null*/) {
     const int acc = 3;
     const int dn = dPML + 2 * acc;
     const int dnx = dn, dny = dn, dny2 = dn;
@@ -397,6 +465,8 @@ void solver_ac(int iprop, int disk_mode, int dPML, int fs, int NumRec,
         for (size_t q = 0; q < (size_t)nt * NumRec; ++q) out[q] = T(0);
 
     const size_t fstride = (size_t)ny * nx;
+    std::vector<T> comp((mo && mo->kahan && iprop == 2) ? fstride : 0, T(0));
+    const T* mixed_w = mixed_weights;
     for (int k = 2; k <= nt; ++k) {
         l = l + 1;
         if (iprop == 1) source(nys[0], nxs[0]) = S[k - 2];
@@ -461,9 +531,36 @@ void solver_ac(int iprop, int disk_mode, int dPML, int fs, int NumRec,
             for (int i = 1; i <= nx; ++i)
                 for (int j = 1; j <= ny; ++j)
                     F[(size_t)(i - 1) * ny + (j - 1)] = ((p_3(dny2 + j, dnx + i) - p_1(dny2 + j, dnx + i)) * T(0.5)) / dt;
+            if (mo) quantize_snapshot<T>(F, fstride, mo->q16);
             l = 0;
         }
-        if (iprop == 2 && l == store_snap) {
+        if (iprop == 2 && mo && mo->pair_mode == 1) {
+            // Mixed form: slot m pairs with backward step k = nt + 1 - store_snap*m.
+            const int r = nt + 1 - k;
+            const int m = (r % store_snap == 0) ? r / store_snap : 0;
+            if (m >= 1 && m <= nt_snap) {
+                const T* F = Fields + (size_t)(m - 1) * fstride;
+                const T ss = T(store_snap);
+                for (int i = 1; i <= nx; ++i)
+                    for (int j = 1; j <= ny; ++j) {
+                        const size_t q = (size_t)(i - 1) * ny + (j - 1);
+                        if (mixed_w && mixed_w[m - 1] == T(0)) continue;
+                        T Fv = F[q];
+                        if (mixed_w && mixed_w[m - 1] != T(1)) Fv = Fv * mixed_w[m - 1];
+                        const T inc = ((T(0.5) * (p_3(dny2 + j, dnx + i) - p_1(dny2 + j, dnx + i))) * Fv) * ss;
+                        T& kk = out[q];
+                        if (mo->kahan) {
+                            T& cc = comp[q];
+                            const T y = inc - cc;
+                            const T t = kk + y;
+                            cc = (t - kk) - y;
+                            kk = t;
+                        } else {
+                            kk = kk + inc;
+                        }
+                    }
+            }
+        } else if (iprop == 2 && l == store_snap) {
             snap = snap - 1;
             const T* F = Fields + (size_t)(snap - 1) * fstride;
             const T ss = T(store_snap);
@@ -553,6 +650,40 @@ void rtm_shot(int disk_mode, int dPML, int fs, int NumRec, int nxSou, int nySou,
     for (size_t q = 0; q < (size_t)ny * nx_w; ++q) PSDM_w[q] = T(0);
     solver_ac<T>(2, disk_mode, dPML, fs, NumRec, nxs.data(), nys.data(), nxr.data(), nyr.data(),
                  back.data(), dd, dt, ny, nx_w, Vp_w, store_snap, nt_taper, nt_taper, Fields.data(), PSDM_w);
+}
+
+// Per-shot RTM in the mixed-precision form (see MixedOpts): forward with
+// snapshots every store_snap steps (quantized in the float build when
+// mo.q16 != 0), taper weights per slot taken at the slot's time sample
+// store_snap*m, time-reversed back-source, backward imaging at the paired
+// steps.  Slots whose weight is zero contribute nothing.
+template <class T>
+void rtm_shot_mixed(const MixedOpts& mo, int disk_mode, int dPML, int fs, int NumRec, int nxSou, int nySou,
+                    const int* nxRec, const int* nyRec, const T* Data_source, const T* Data_target, T dd, T dt,
+                    int ny, int nx, int nx_w, const T* Vp_w, float added_space, int store_snap, int nt_prop2,
+                    int nt_taper, int taper_option, int N_taper, int N_zeros, T* PSDM_w, T* Fields_out) {
+    int nxw2, xi, xf;
+    dynamic_window(NumRec, nxSou, nxRec, (float)dd, nx, added_space, &nxw2, &xi, &xf);
+    std::vector<int> nxs{nxSou - xi + 1}, nys{nySou}, nxr(NumRec), nyr(NumRec);
+    for (int r = 0; r < NumRec; ++r) { nxr[r] = nxRec[r] - xi + 1; nyr[r] = nyRec[r]; }
+    const int nsnap = (nt_prop2 - 1) / store_snap;
+    const size_t fs2 = (size_t)ny * nx_w;
+    std::vector<T> Fields(fs2 * std::max(nsnap, 1), T(0));
+    std::vector<T> synth((size_t)nt_prop2 * NumRec, T(0));
+    solver_ac<T>(1, disk_mode, dPML, fs, NumRec, nxs.data(), nys.data(), nxr.data(), nyr.data(), Data_source, dd,
+                 dt, ny, nx_w, Vp_w, store_snap, nsnap, nt_prop2, Fields.data(), synth.data(), nullptr, &mo);
+    if (Fields_out) std::copy(Fields.begin(), Fields.begin() + fs2 * nsnap, Fields_out);
+    std::vector<T> wts(nt_taper, T(1));
+    if (taper_option != 0) taper_pad_trace<T>(wts.data(), nt_prop2, N_taper, N_zeros, nt_taper);
+    std::vector<T> wslot(std::max(nsnap, 1), T(1));
+    for (int m = 1; m <= nsnap; ++m) wslot[m - 1] = wts[(size_t)store_snap * m - 1];
+    std::vector<T> back((size_t)nt_taper * NumRec);
+    for (int r = 0; r < NumRec; ++r)
+        for (int t = 0; t < nt_taper; ++t)
+            back[(size_t)r * nt_taper + t] = Data_target[(size_t)r * nt_taper + (nt_taper - 1 - t)];
+    for (size_t q = 0; q < fs2; ++q) PSDM_w[q] = T(0);
+    solver_ac<T>(2, disk_mode, dPML, fs, NumRec, nxs.data(), nys.data(), nxr.data(), nyr.data(), back.data(), dd,
+                 dt, ny, nx_w, Vp_w, store_snap, nsnap, nt_taper, Fields.data(), PSDM_w, nullptr, &mo, wslot.data());
 }
 
 template <class T>
@@ -658,6 +789,40 @@ void orc_rtm_shot_d(int disk_mode, int dPML, int fs, int NumRec, int nxSou, int 
     rtm_shot<double>(disk_mode, dPML, fs, NumRec, nxSou, nySou, nxRec, nyRec, src.data(), tgt.data(), double(dd),
                      double(dt), ny, nx, nx_w, vp.data(), added_space, store_snap, nt_snap, nt_prop2, nt_taper,
                      taper_option, N_taper, N_zeros, PSDM_w, Data_synth);
+}
+
+// Mixed-precision form, float build: emulates the engine's FP16/BF16 form
+// bit for bit (q16 = 1 / 2, Kahan image).  Fields_out (ny, nx_w, nsnap) gets
+// the snapshots as the backward pass reads them, or null.
+void orc_rtm_shot_mixed_f(int q16, int kahan, int disk_mode, int dPML, int fs, int NumRec, int nxSou, int nySou,
+                          const int* nxRec, const int* nyRec, const float* Data_source, const float* Data_target,
+                          float dd, float dt, int ny, int nx, int nx_w, const float* Vp_w, float added_space,
+                          int store_snap, int nt_prop2, int nt_taper, int taper_option, int N_taper, int N_zeros,
+                          float* PSDM_w, float* Fields_out) {
+    MixedOpts mo;
+    mo.pair_mode = 1;
+    mo.q16 = q16;
+    mo.kahan = kahan;
+    rtm_shot_mixed<float>(mo, disk_mode, dPML, fs, NumRec, nxSou, nySou, nxRec, nyRec, Data_source, Data_target, dd,
+                          dt, ny, nx, nx_w, Vp_w, added_space, store_snap, nt_prop2, nt_taper, taper_option, N_taper,
+                          N_zeros, PSDM_w, Fields_out);
+}
+
+// Mixed-precision form, FP64 oracle: the same schedule in double precision
+// throughout (no rounding of the snapshots, plain summation).
+void orc_rtm_shot_mixed_d(int disk_mode, int dPML, int fs, int NumRec, int nxSou, int nySou, const int* nxRec,
+                          const int* nyRec, const float* Data_source, const float* Data_target, float dd, float dt,
+                          int ny, int nx, int nx_w, const float* Vp_w, float added_space, int store_snap,
+                          int nt_prop2, int nt_taper, int taper_option, int N_taper, int N_zeros, double* PSDM_w,
+                          double* Fields_out) {
+    MixedOpts mo;
+    mo.pair_mode = 1;
+    auto src = widen<double>(Data_source, (size_t)nt_prop2);
+    auto tgt = widen<double>(Data_target, (size_t)nt_taper * NumRec);
+    auto vp = widen<double>(Vp_w, (size_t)ny * nx_w);
+    rtm_shot_mixed<double>(mo, disk_mode, dPML, fs, NumRec, nxSou, nySou, nxRec, nyRec, src.data(), tgt.data(),
+                           double(dd), double(dt), ny, nx, nx_w, vp.data(), added_space, store_snap, nt_prop2,
+                           nt_taper, taper_option, N_taper, N_zeros, PSDM_w, Fields_out);
 }
 
 // src/auxiliar_PSDM.f90:1-20.
