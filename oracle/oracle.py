@@ -62,6 +62,11 @@ def lib():
         L.orc_rtm_shot_f.argtypes = shot_args + [_f32p, C.c_void_p]
         L.orc_rtm_shot_d.argtypes = shot_args + [_f64p, C.c_void_p]
         L.orc_normalize_psdm.argtypes = [_I, _I, _f32p, _f32p, _f32p]
+        # disk_mode .. N_zeros without nt_snap (mixed form)
+        mixed_args = [_I, _I, _I, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F,
+                      _I, _I, _I, _I, _I, _I]
+        L.orc_rtm_shot_mixed_f.argtypes = [_I, _I] + mixed_args + [_f32p, C.c_void_p]
+        L.orc_rtm_shot_mixed_d.argtypes = mixed_args + [_f64p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -172,6 +177,33 @@ def rtm_shot(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, Data_s
        added_space, store_snap, nt_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, img,
        synth.ctypes.data if synth is not None else None)
     return (img, synth) if want_synth else img
+
+
+def rtm_shot_mixed(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target,
+                   dd: float, dt: float, nx: int, vp_w, added_space: float, store_snap: int, nt_prop2: int,
+                   nt_taper: int, taper_option: int = 0, N_taper: int = 1, N_zeros: int = 0, disk_mode: int = 0,
+                   q16: int = 0, kahan: int = 1, dtype=np.float32, want_fields: bool = False):
+    """The engine's mixed-precision form for one shot (no reference
+    counterpart): snapshots every store_snap steps, imaging at the paired
+    backward steps.  float32: emulation of the engine (q16 = 1 binary16,
+    2 bfloat16, 0 unrounded; Kahan image if kahan); float64: the FP64 oracle
+    of the form (q16 and kahan ignored).  Returns the image (nx_w, ny) and, if
+    asked, the snapshots as read back (nsnap, nx_w, ny)."""
+    vp_w = _f32(vp_w)
+    nx_w, ny = vp_w.shape
+    nrec = len(np.atleast_1d(nxRec))
+    nsnap = (nt_prop2 - 1) // store_snap
+    img = np.zeros((nx_w, ny), dtype=dtype)
+    F = np.zeros((max(nsnap, 1), nx_w, ny), dtype=dtype) if want_fields else None
+    args = [disk_mode, dPML, fs, nrec, int(nxSou), int(nySou), _i32(nxRec), _i32(nyRec),
+            _f32(Data_source).reshape(-1), _f32(Data_target).reshape(-1), dd, dt, ny, nx, nx_w, vp_w,
+            added_space, store_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, img,
+            F.ctypes.data if F is not None else None]
+    if dtype == np.float32:
+        lib().orc_rtm_shot_mixed_f(q16, kahan, *args)
+    else:
+        lib().orc_rtm_shot_mixed_d(*args)
+    return (img, F[:nsnap]) if want_fields else img
 
 
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:

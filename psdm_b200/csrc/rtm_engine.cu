@@ -78,7 +78,7 @@ struct psdm_engine {
     struct GraphCache {
         std::vector<StepArgs> args;
         cudaGraphExec_t exec = nullptr;
-    } graphs[2];
+    } graphs[3];
     bool use_graphs = true;
     int batch_slots = 0;  // slots used by the last batched call
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
@@ -593,6 +593,130 @@ int window_geometry(const Grid& g, int NumRec, int nxSou, int nySou, const int* 
     return PSDM_OK;
 }
 
+// ---- mixed-precision form ----------------------------------------------------
+//
+// prm->precision = PSDM_PREC_FP16 / _BF16.  Propagation is the same FP32
+// step; the forward pass keeps a snapshot every store_snap steps as 16-bit
+// values scaled by a power of two chosen from that snapshot's largest
+// magnitude (the snapshot is written in FP32 to a staging buffer with its
+// maximum, and converted by the next step's launch), and the backward pass
+// images at the steps paired in time with the stored snapshots,
+// k_b = nt_taper + 1 - store_snap*m for slot m, summing the image with Kahan
+// compensation.  The taper weight of slot m is the weight of its time
+// sample store_snap*m.  This form has no reference counterpart; for
+// store_snap = 1 its pairing is the reference's.
+
+struct MixedBufs {
+    int kind = 0;  // 1 binary16, 2 bfloat16
+    int ks = 1;    // snapshot interval (store_snap)
+    int nsnap = 0;
+    size_t fstride = 0;
+    float* stage[2] = {nullptr, nullptr};
+    unsigned int* amax = nullptr;  // nsnap
+    unsigned short* snap16 = nullptr;  // nsnap * fstride
+    float* iscale = nullptr;       // nsnap
+    float* comp = nullptr;         // fstride
+};
+
+int mixed_bufs(psdm_engine* e, const Shot& s, int kind, int ks, int nt_prop2, const std::string& tag, MixedBufs* mb) {
+    mb->kind = kind;
+    mb->ks = ks;
+    mb->nsnap = (nt_prop2 - 1) / ks;
+    mb->fstride = s.g.field_cells();
+    const size_t fs = mb->fstride, ns = (size_t)std::max(mb->nsnap, 1);
+    TRY(e->get(("stage0" + tag).c_str(), fs, &mb->stage[0]));
+    TRY(e->get(("stage1" + tag).c_str(), fs, &mb->stage[1]));
+    TRY(e->get(("amax" + tag).c_str(), ns, &mb->amax));
+    TRY(e->get(("snap16" + tag).c_str(), ns * fs, &mb->snap16));
+    TRY(e->get(("iscale" + tag).c_str(), ns, &mb->iscale));
+    TRY(e->get(("comp" + tag).c_str(), fs, &mb->comp));
+    // The staging buffers' pad rows are converted too: keep them zero.
+    CUDA_TRY(cudaMemsetAsync(mb->stage[0], 0, fs * sizeof(float), e->stream));
+    CUDA_TRY(cudaMemsetAsync(mb->stage[1], 0, fs * sizeof(float), e->stream));
+    CUDA_TRY(cudaMemsetAsync(mb->amax, 0, ns * sizeof(unsigned int), e->stream));
+    CUDA_TRY(cudaMemsetAsync(mb->comp, 0, fs * sizeof(float), e->stream));
+    return PSDM_OK;
+}
+
+// Forward steps (k = 2..nt) of the mixed form: snapshot slot m at the steps
+// with (k-1) % ks == 0, each converted by the following step.  *pending =
+// the slot taken at the last step (to be converted after the pass), or 0.
+void mixed_forward_args(const MixedBufs& mb, std::vector<StepArgs>& steps, size_t first, int* pending) {
+    int prev = 0;
+    for (size_t i = first; i < steps.size(); ++i) {
+        StepArgs& a = steps[i];
+        const int k = (int)(i - first) + 2;
+        a.kind16 = mb.kind;
+        a.field = nullptr;
+        a.field_amax = nullptr;
+        a.q_src = nullptr;
+        if (prev > 0) {
+            a.q_src = mb.stage[prev & 1];
+            a.q_amax = mb.amax + (prev - 1);
+            a.q_dst = mb.snap16 + (size_t)(prev - 1) * mb.fstride;
+            a.q_iscale = mb.iscale + (prev - 1);
+            a.q_n = (int)mb.fstride;
+            prev = 0;
+        }
+        if ((k - 1) % mb.ks == 0) {
+            const int m = (k - 1) / mb.ks;
+            if (m >= 1 && m <= mb.nsnap) {
+                a.field = mb.stage[m & 1];
+                a.field_amax = mb.amax + (m - 1);
+                prev = m;
+            }
+        }
+    }
+    *pending = prev;
+}
+
+int mixed_quantize(psdm_engine* e, const MixedBufs& mb, int m) {
+    if (m <= 0) return PSDM_OK;
+    const int rc = launch_quantize(mb.stage[m & 1], mb.amax + (m - 1), mb.snap16 + (size_t)(m - 1) * mb.fstride,
+                                   mb.iscale + (m - 1), (int)mb.fstride, mb.kind, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "snapshot conversion launch: %s", cudaGetErrorString((cudaError_t)rc));
+    e->launches += 1;
+    return PSDM_OK;
+}
+
+// Backward steps (k = 2..nt) of the mixed form: slot m pairs with
+// k = nt + 1 - ks*m; h_w = per-sample taper weights (nt entries) or null.
+void mixed_backward_args(const MixedBufs& mb, int nt, const float* h_w, std::vector<StepArgs>& steps,
+                         size_t first) {
+    for (size_t i = first; i < steps.size(); ++i) {
+        StepArgs& a = steps[i];
+        const int k = (int)(i - first) + 2;
+        a.kind16 = mb.kind;
+        a.field = nullptr;
+        a.field16 = nullptr;
+        a.comp = mb.comp;
+        a.ss = float(mb.ks);
+        a.field_w = 1.f;
+        const int r = nt + 1 - k;
+        if (r % mb.ks != 0) continue;
+        const int m = r / mb.ks;
+        if (m < 1 || m > mb.nsnap) continue;
+        const float w = h_w ? h_w[(size_t)mb.ks * m - 1] : 1.f;
+        if (w == 0.f) continue;  // zero weight: no contribution
+        a.field16 = mb.snap16 + (size_t)(m - 1) * mb.fstride;
+        a.field_iscale = mb.iscale + (m - 1);
+        a.field_w = w;
+    }
+}
+
+// Per-sample taper weights of the snapshot series (calculate_PSDM_RTM.f90:421-427).
+std::vector<float> taper_weights(int nt_prop2, int nt_taper, int taper_option, int N_taper, int N_zeros) {
+    std::vector<float> wts(std::max(nt_taper, 1), 1.f);
+    if (taper_option != 0) {
+        const int i0 = std::max(1, nt_prop2 - N_taper + 1);
+        for (int n = 0; n < N_taper; ++n)
+            if (i0 + n <= nt_prop2) wts[i0 + n - 1] = taper_weight(n, N_taper);
+        if (N_zeros > 0)
+            for (int i = nt_prop2; i < nt_taper; ++i) wts[i] = 0.f;
+    }
+    return wts;
+}
+
 // One shot of RTM with every array in device memory
 // (calculate_PSDM_RTM.f90:395-466).  Asynchronous on e->stream.
 int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
@@ -600,7 +724,8 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
                   int nx_w, const float* d_vp, float added_space, int store_snap, int nt_snap, int nt_prop2,
                   int nt_taper, int taper_option, int N_taper, int N_zeros, float* d_img) {
     TRY(check_params(prm));
-    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (prm->precision != PSDM_PREC_FP32 && prm->precision != PSDM_PREC_FP16 && prm->precision != PSDM_PREC_BF16)
+        return fail(PSDM_ERR_ARG, "unknown precision %d", prm->precision);
     if (NumRec < 1 || !nxRec || !nyRec || !d_S || !d_tgt || !d_vp || !d_img)
         return fail(PSDM_ERR_ARG, "null argument or NumRec < 1");
     if (nt_prop2 < 2 || nt_taper < 2 || store_snap < 1 || nt_taper < nt_prop2)
@@ -616,8 +741,36 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
         return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
     const size_t fstride = s.g.field_cells();
     float *d_F = nullptr, *d_imgp = nullptr;
-    if (nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
     TRY(e->get("image_pitched", fstride, &d_imgp));
+    if (prm->precision != PSDM_PREC_FP32) {
+        MixedBufs mb;
+        TRY(mixed_bufs(e, s, prm->precision, store_snap, nt_prop2, "", &mb));
+        TRY(e->record(0));
+        std::vector<StepArgs> fw;
+        TRY(build_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, "", &fw));
+        int pending = 0;
+        mixed_forward_args(mb, fw, 0, &pending);
+        TRY(launch_steps(e, 0, fw));
+        e->launches += nt_prop2 - 1;
+        e->fwd_steps += nt_prop2 - 1;
+        TRY(mixed_quantize(e, mb, pending));
+        TRY(e->record(1));
+        const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, taper_option, N_taper, N_zeros);
+        CUDA_TRY(cudaMemsetAsync(d_imgp, 0, fstride * sizeof(float), e->stream));
+        TRY(reset_state(e, &s));
+        std::vector<StepArgs> bw;
+        TRY(build_backward(e, s, nt_taper, store_snap, nt_taper, d_tgt, 1, NumRec, w.zr.data(), w.xr.data(), nullptr,
+                           1, 0, nullptr, d_imgp, "", &bw));
+        mixed_backward_args(mb, nt_taper, wts.data(), bw, 0);
+        TRY(launch_steps(e, 2, bw));
+        e->launches += nt_taper - 1;
+        e->bwd_steps += nt_taper - 1;
+        TRY(e->record(2));
+        CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
+                                   (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
+        return PSDM_OK;
+    }
+    if (nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
     TRY(e->record(0));
     TRY(run_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr));
     TRY(e->record(1));
@@ -669,6 +822,9 @@ struct BatchSlot {
     float* h_out = nullptr;      // host variant: caller's image, pending copy-out
     int out_ny = 0, out_nx = 0;
     cudaEvent_t staged = nullptr;  // the slot's page-locked staging is free again
+    int bwd_mode = 1;              // 1 plain backward, 2 mixed-precision backward
+    MixedBufs mb;                  // mixed form: the slot's 16-bit snapshots
+    int pending = 0;               // mixed form: slot taken at the last forward step
 };
 
 struct BatchJob {
@@ -723,24 +879,24 @@ int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
     const int nt_prop2 = sh.nt_prop2, nt_taper = sh.nt_taper;
     const int nsnap = (nt_prop2 - 1) / j.store_snap;
     const size_t fstride = sl.s.g.field_cells();
+    const bool mixed = j.prm->precision != PSDM_PREC_FP32;
     float* d_F = nullptr;
-    if (nsnap > 0) TRY(e->get(("fields" + tag).c_str(), fstride * nsnap, &d_F));
+    if (mixed)
+        TRY(mixed_bufs(e, sl.s, j.prm->precision, j.store_snap, nt_prop2, tag, &sl.mb));
+    else if (nsnap > 0)
+        TRY(e->get(("fields" + tag).c_str(), fstride * nsnap, &d_F));
     TRY(e->get(("imgp" + tag).c_str(), fstride, &sl.d_imgp));
-    // Taper of the snapshot series, as in rtm_shot_core.
-    std::vector<float> wts(std::max(nt_taper, 1), 1.f);
-    if (j.taper_option != 0) {
-        const int i0 = std::max(1, nt_prop2 - j.N_taper + 1);
-        for (int n = 0; n < j.N_taper; ++n)
-            if (i0 + n <= nt_prop2) wts[i0 + n - 1] = taper_weight(n, j.N_taper);
-        if (j.N_zeros > 0)
-            for (int t = nt_prop2; t < nt_taper; ++t) wts[t] = 0.f;
-    }
+    const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, j.taper_option, j.N_taper, j.N_zeros);
     std::vector<StepArgs> steps;
     TRY(build_forward(e, sl.s, nt_prop2, j.store_snap, j.d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr, tag,
                       &steps));
     sl.nfwd = (int)steps.size();
+    sl.pending = 0;
+    if (mixed) mixed_forward_args(sl.mb, steps, 0, &sl.pending);
     TRY(build_backward(e, sl.s, nt_taper, j.store_snap, nt_taper, d_tgt, 1, sh.NumRec, w.zr.data(), w.xr.data(),
                        d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps));
+    if (mixed) mixed_backward_args(sl.mb, nt_taper, wts.data(), steps, (size_t)sl.nfwd);
+    sl.bwd_mode = mixed ? 2 : 1;
     sl.nbwd = (int)steps.size() - sl.nfwd;
     sl.tiles[0] = sl.nfwd > 0 ? steps[0].r_first[steps[0].nrect] : 0;
     sl.tiles[1] = sl.nbwd > 0 ? steps[sl.nfwd].r_first[steps[sl.nfwd].nrect] : 0;
@@ -803,8 +959,10 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         TRY(build_grid(j.prm, j.ny, j.shots[i].nx_w, &g));
         const size_t nsnap = (size_t)(j.shots[i].nt_prop2 - 1) / j.store_snap;
         const size_t steps = (size_t)j.shots[i].nt_prop2 + j.shots[i].nt_taper;
-        size_t b = 9 * g.cells() * sizeof(float) + (nsnap + 1) * g.field_cells() * sizeof(float) +
-                   steps * sizeof(StepArgs);
+        const size_t snap_bytes = j.prm->precision != PSDM_PREC_FP32
+                                      ? (nsnap * 2 + 4 * 4) * g.field_cells()   // 16-bit slots, 2 stages, comp, image
+                                      : (nsnap + 1) * g.field_cells() * sizeof(float);
+        size_t b = 9 * g.cells() * sizeof(float) + snap_bytes + steps * sizeof(StepArgs);
         if (j.host_io) b += ((size_t)j.ny * j.shots[i].nx_w + (size_t)j.shots[i].NumRec * j.shots[i].nt_taper) *
                             sizeof(float);
         per_slot = std::max(per_slot, b);
@@ -855,7 +1013,7 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         int n = 0;
         for (BatchSlot& sl : slots) {
             if (sl.shot < 0) continue;
-            bp.mode[n] = sl.pass;
+            bp.mode[n] = sl.pass == 0 ? 0 : sl.bwd_mode;
             bp.args[n] = sl.d_args + (sl.pass == 0 ? sl.k : sl.nfwd + sl.k);
             bp.first[n + 1] = bp.first[n] + sl.tiles[sl.pass];
             ++n;
@@ -878,7 +1036,8 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
                 e->fwd_steps += 1;
                 if (sl.k < sl.nfwd) continue;
                 // Second propagator call on the same model: fresh wavefield.
-                rc = reset_state(e, &sl.s);
+                if (sl.bwd_mode == 2) rc = mixed_quantize(e, sl.mb, sl.pending);
+                if (rc == PSDM_OK) rc = reset_state(e, &sl.s);
                 sl.pass = 1;
                 sl.k = 0;
                 if (rc != PSDM_OK) break;
@@ -1146,7 +1305,8 @@ int psdm_rtm_batch(psdm_engine* e, const psdm_params* prm, int32_t nshots, const
                    int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots) {
     TRY(check_engine(e));
     TRY(check_params(prm));
-    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (prm->precision != PSDM_PREC_FP32 && prm->precision != PSDM_PREC_FP16 && prm->precision != PSDM_PREC_BF16)
+        return fail(PSDM_ERR_ARG, "unknown precision %d", prm->precision);
     if (nshots < 0 || (nshots > 0 && (!shots || !Data_source))) return fail(PSDM_ERR_ARG, "null argument");
     if (store_snap < 1) return fail(PSDM_ERR_ARG, "store_snap must be >= 1");
     if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
@@ -1166,7 +1326,8 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
                           int32_t max_slots) {
     TRY(check_engine(e));
     TRY(check_params(prm));
-    if (prm->precision != PSDM_PREC_FP32) return fail(PSDM_ERR_ARG, "mixed precision is not built yet");
+    if (prm->precision != PSDM_PREC_FP32 && prm->precision != PSDM_PREC_FP16 && prm->precision != PSDM_PREC_BF16)
+        return fail(PSDM_ERR_ARG, "unknown precision %d", prm->precision);
     if (nshots < 0 || (nshots > 0 && (!shots || !d_Data_source))) return fail(PSDM_ERR_ARG, "null argument");
     if (store_snap < 1) return fail(PSDM_ERR_ARG, "store_snap must be >= 1");
     if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");

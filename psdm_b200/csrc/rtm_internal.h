@@ -91,10 +91,25 @@ struct StepArgs {
     int counter_sel;
     int num_sms;
     int* err;  // set to 1 if a bulk copy did not complete
+    // Mixed-precision form: snapshots kept as binary16 / bfloat16 scaled by a
+    // power of two per snapshot, image summed with Kahan compensation.
+    unsigned int* field_amax;   // forward: max |snapshot| of this step (float bits), or null
+    const void* field16;        // backward (mode 2): this step's 16-bit snapshot, pitched like field
+    const float* field_iscale;  // its inverse scale 2^-k
+    float* comp;                // backward (mode 2): Kahan compensation of the image
+    int kind16;                 // 1 = binary16, 2 = bfloat16
+    // Quantization of an earlier snapshot, done by this launch's blocks
+    // before their tiles: q_dst[i] = round16(q_src[i] * 2^k) for i < q_n and
+    // *q_iscale = 2^-k, with k from *q_amax.  q_src = null: none.
+    int q_n;
+    const float* q_src;
+    const unsigned int* q_amax;
+    void* q_dst;
+    float* q_iscale;
 };
 
 // One launch advancing several shots ("slots") by one time step each:
-// slot s runs pass mode[s] (0 forward, 1 backward) with the step arguments
+// slot s runs pass mode[s] (0 forward, 1 backward, 2 mixed backward) with the step arguments
 // at args[s] (device memory); its tiles are [first[s], first[s+1]) of the
 // launch's work list, first[s+1] - first[s] = that step's r_first[nrect].
 // counter[counter_sel] starts at 0; the launch clears the other one.
@@ -116,8 +131,12 @@ void plan_tiles(StepArgs* a, const int* row_slot_host);
 // Set kernel attributes (shared memory carve-out, occupancy); call once per
 // device before the first launch.  Returns a cudaError_t value.
 int prepare_step_kernels();
-// Launch one fused forward (mode 0) or backward (mode 1) step on `stream`.
+// Launch one fused forward (mode 0), backward (mode 1) or mixed-precision
+// backward (mode 2: 16-bit snapshots, Kahan image) step on `stream`.
 int launch_step(int mode, const StepArgs& a, void* stream);
+// Quantize one snapshot outside a step launch (see StepArgs::q_*).
+int launch_quantize(const float* src, const unsigned int* amax, void* dst, float* iscale, int n, int kind16,
+                    void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.
 int launch_batch_step(const BatchParams& bp, int num_sms, void* stream);
 // Receiver gather after the last forward step (Rec(nt-1) and Rec(nt)).

@@ -39,6 +39,8 @@
 // Memory: p1 is overwritten in place with p3; phi is ping-ponged because its
 // strip stencil reads neighbours; chi is updated in place.
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -118,6 +120,77 @@ __device__ __forceinline__ float div_dt(const StepArgs& a, float x) {
 
 __device__ __forceinline__ float comp(const float4& v, int r) {
     return r == 0 ? v.x : (r == 1 ? v.y : (r == 2 ? v.z : v.w));
+}
+
+// ---- mixed-precision form: 16-bit snapshots and Kahan image -------------------
+
+// Largest |snapshot| seen by this block since the last flush (float bits; the
+// order of non-negative floats is the order of their bit patterns).
+__shared__ unsigned int s_blk_amax;
+
+__device__ __forceinline__ void amax_note(float v) { atomicMax(&s_blk_amax, __float_as_uint(fabsf(v))); }
+
+// Scale exponent k for a snapshot of largest magnitude A (bits): A * 2^k in
+// [2^14, 2^15), clamped to [-126, 126]; k = 0 for an all-zero snapshot.
+__device__ __forceinline__ int snapshot_scale_exp(unsigned int bits) {
+    if (bits == 0u) return 0;
+    const int e = (int)((bits >> 23) & 0xffu) - 127;
+    return min(126, max(-126, 14 - e));
+}
+__device__ __forceinline__ float pow2f(int k) { return __uint_as_float((unsigned int)(k + 127) << 23); }
+
+// q_dst[i] = round16(q_src[i] * 2^k), i < n (n a multiple of 4), over the
+// launch's blocks; block 0 writes 2^-k.
+__device__ __forceinline__ void quantize_part(const float* __restrict__ src, const unsigned int* amax, void* dst,
+                                              float* iscale, int n, int kind16, int tid) {
+    const int k = snapshot_scale_exp(__ldg(amax));
+    const float sc = pow2f(k);
+    if (blockIdx.x == 0 && tid == 0) *iscale = pow2f(-k);
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    uint2* d4 = reinterpret_cast<uint2*>(dst);
+    for (int i = blockIdx.x * NT + tid; i < n / 4; i += gridDim.x * NT) {
+        const float4 v = __ldg(s4 + i);
+        const float x0 = __fmul_rn(v.x, sc), x1 = __fmul_rn(v.y, sc), x2 = __fmul_rn(v.z, sc),
+                    x3 = __fmul_rn(v.w, sc);
+        uint2 o;
+        if (kind16 == 1) {
+            const __half2 a = __floats2half2_rn(x0, x1), b = __floats2half2_rn(x2, x3);
+            o.x = *reinterpret_cast<const unsigned int*>(&a);
+            o.y = *reinterpret_cast<const unsigned int*>(&b);
+        } else {
+            const __nv_bfloat162 a = __floats2bfloat162_rn(x0, x1), b = __floats2bfloat162_rn(x2, x3);
+            o.x = *reinterpret_cast<const unsigned int*>(&a);
+            o.y = *reinterpret_cast<const unsigned int*>(&b);
+        }
+        d4[i] = o;
+    }
+}
+
+__device__ __forceinline__ float2 unpack16(unsigned int w, int kind16) {
+    if (kind16 == 1) return __half22float2(*reinterpret_cast<const __half2*>(&w));
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w));
+}
+
+// Four consecutive snapshot values (16-byte aligned group) as floats.
+__device__ __forceinline__ float4 load16x4(const void* base, int fi, int kind16, float isc) {
+    const uint2 w = __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + fi));
+    const float2 a = unpack16(w.x, kind16), b = unpack16(w.y, kind16);
+    return make_float4(__fmul_rn(a.x, isc), __fmul_rn(a.y, isc), __fmul_rn(b.x, isc), __fmul_rn(b.y, isc));
+}
+
+__device__ __forceinline__ float load16x1(const void* base, int fi, int kind16, float isc) {
+    const unsigned short h = __ldg(static_cast<const unsigned short*>(base) + fi);
+    const float v = kind16 == 1 ? __half2float(__ushort_as_half(h)) : __bfloat162float(__ushort_as_bfloat16(h));
+    return __fmul_rn(v, isc);
+}
+
+// img += inc with Kahan compensation c: y = inc - c, t = img + y,
+// c = (t - img) - y, img = t.
+__device__ __forceinline__ void kahan(float& img, float& c, float inc) {
+    const float y = __fsub_rn(inc, c);
+    const float t = __fadd_rn(img, y);
+    c = __fsub_rn(__fsub_rn(t, img), y);
+    img = t;
 }
 
 // ---- bulk asynchronous copies (global -> shared) completing on an mbarrier
@@ -273,7 +346,9 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
     if (kx == 0 && kz == 0 && a.field != nullptr) {
         const int fi = (x - dn) * a.ldf + (z - dn);
         if (MODE == 0) {
-            a.field[fi] = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
+            const float D = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
+            a.field[fi] = D;
+            if (a.field_amax != nullptr) amax_note(D);
         } else {
             float F = __ldg(a.field + fi);
             if (a.field_w != 1.f) F = __fmul_rn(F, a.field_w);
@@ -281,6 +356,14 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
             if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
             a.image[fi] = __fadd_rn(a.image[fi], inc);
         }
+    }
+    if (MODE == 2 && kx == 0 && kz == 0 && a.field16 != nullptr) {
+        const int fi = (x - dn) * a.ldf + (z - dn);
+        float F = load16x1(a.field16, fi, a.kind16, __ldg(a.field_iscale));
+        if (a.field_w != 1.f) F = __fmul_rn(F, a.field_w);
+        float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
+        if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+        kahan(a.image[fi], a.comp[fi], inc);
     }
 }
 
@@ -351,11 +434,19 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     const int z = zd - a.zoff;
     int fi = (x0 + c0 - dn) * a.ldf + (z - dn);
     const bool img = MODE == 1 && a.field != nullptr;
-    float4 Fn = make_float4(0.f, 0.f, 0.f, 0.f), In = Fn;
+    const bool img16 = MODE == 2 && a.field16 != nullptr;
+    const float isc = img16 ? __ldg(a.field_iscale) : 1.f;
+    float4 Fn = make_float4(0.f, 0.f, 0.f, 0.f), In = Fn, Cn = Fn;
     if (img && active) {  // first column of the snapshot and image, while the copies land
         Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi));
         In = *reinterpret_cast<const float4*>(a.image + fi);
     }
+    if (img16 && active) {
+        Fn = load16x4(a.field16, fi, a.kind16, isc);
+        In = *reinterpret_cast<const float4*>(a.image + fi);
+        Cn = *reinterpret_cast<const float4*>(a.comp + fi);
+    }
+    float amax_t = 0.f;
     const bool ok = mbar_wait_bounded(bar, phase);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -384,10 +475,15 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         const float4 zp = ps4[(col + 3) * HQ + qr + 1];
         const float4 pmv = *reinterpret_cast<const float4*>(pms + col * TZ + q);
         const float4 c2v = *reinterpret_cast<const float4*>(c2s + col * TZ + q);
-        float4 Fc = Fn, Ic = In;
+        float4 Fc = Fn, Ic = In, Cc = Cn;
         if (img && c + 1 < ncol) {  // next column of the snapshot and image
             Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi + a.ldf));
             In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
+        }
+        if (img16 && c + 1 < ncol) {
+            Fn = load16x4(a.field16, fi + a.ldf, a.kind16, isc);
+            In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
+            Cn = *reinterpret_cast<const float4*>(a.comp + fi + a.ldf);
         }
         const float4& pc = win[3];
         // z-window rows -3..+6 around the float4: pairs (i, i+1) of
@@ -426,6 +522,25 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
             sv.z = div_dt(a, __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f));
             sv.w = div_dt(a, __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f));
             *reinterpret_cast<float4*>(a.field + fi) = sv;
+            if (a.field_amax != nullptr)
+                amax_t = fmaxf(amax_t, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(sv.z), fabsf(sv.w))));
+        }
+        if (MODE == 2 && img16) {
+            float Fv[4] = {Fc.x, Fc.y, Fc.z, Fc.w};
+            float Iv[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
+            float Cv[4] = {Cc.x, Cc.y, Cc.z, Cc.w};
+            const float ov[4] = {out.x, out.y, out.z, out.w};
+            const float pv[4] = {pmv.x, pmv.y, pmv.z, pmv.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float F = Fv[e];
+                if (a.field_w != 1.f) F = __fmul_rn(F, a.field_w);
+                float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(ov[e], pv[e])), F);
+                if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+                kahan(Iv[e], Cv[e], inc);
+            }
+            *reinterpret_cast<float4*>(a.image + fi) = make_float4(Iv[0], Iv[1], Iv[2], Iv[3]);
+            *reinterpret_cast<float4*>(a.comp + fi) = make_float4(Cv[0], Cv[1], Cv[2], Cv[3]);
         }
         if (MODE == 1 && img) {
             if (a.field_w != 1.f) {
@@ -448,6 +563,7 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         g += a.ldz;
         fi += a.ldf;
     }
+    if (MODE == 0 && a.field_amax != nullptr && a.field != nullptr) amax_note(amax_t);
     return true;
 }
 
@@ -651,12 +767,16 @@ __global__ void __launch_bounds__(NT) step_kernel(const StepArgs a) {
     __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_id;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    if (tid == 0) mbar_init(&bar, 1);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        s_blk_amax = 0u;
+    }
     if (MODE == 0 && a.rec_t >= 0) {
         // Receivers of the previous step: p is that step's p3.
         for (int i = blockIdx.x * NT + tid; i < a.nrec; i += gridDim.x * NT)
             a.rec_out[(size_t)i * a.rec_ld + a.rec_t] = a.p[a.rec_cell[i]];
     }
+    if (MODE == 0 && a.q_src != nullptr) quantize_part(a.q_src, a.q_amax, a.q_dst, a.q_iscale, a.q_n, a.kind16, tid);
     // Persistent blocks take tiles in order (heaviest rect types first) from
     // this step's counter; the other counter is cleared for the next step.
     if (blockIdx.x == 0 && tid == 0) a.tile_counter[a.counter_sel ^ 1] = 0;
@@ -667,7 +787,11 @@ __global__ void __launch_bounds__(NT) step_kernel(const StepArgs a) {
         if (tid == 0) tile_id = atomicAdd(a.tile_counter + a.counter_sel, 1);
         __syncthreads();
         const int b = tile_id;
-        if (b >= total) return;
+        if (b >= total) {
+            if (MODE == 0 && tid == 0 && a.field_amax != nullptr && s_blk_amax != 0u)
+                atomicMax(a.field_amax, s_blk_amax);
+            return;
+        }
         int r = 0;
         while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
         const int t = b - a.r_first[r];
@@ -713,11 +837,17 @@ __global__ void __launch_bounds__(NT) batch_step_kernel(const BatchParams bp) {
     __shared__ int tile_id;
     __shared__ __align__(16) StepArgs sa;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    if (tid == 0) mbar_init(&bar, 1);
-    // Deferred receiver gathers of the forward slots (p = previous step's p3).
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        s_blk_amax = 0u;
+    }
+    // Deferred receiver gathers of the forward slots (p = previous step's p3),
+    // and their pending snapshot quantizations.
     for (int s = 0; s < bp.nslots; ++s) {
         if (bp.mode[s] != 0) continue;
         const StepArgs* g = bp.args[s];
+        const float* qs = g->q_src;
+        if (qs != nullptr) quantize_part(qs, g->q_amax, g->q_dst, g->q_iscale, g->q_n, g->kind16, tid);
         const int rec_t = g->rec_t, nrec = g->nrec;
         if (rec_t < 0 || nrec <= 0) continue;
         const float* p = g->p;
@@ -738,10 +868,18 @@ __global__ void __launch_bounds__(NT) batch_step_kernel(const BatchParams bp) {
         if (tid == 0) tile_id = atomicAdd(bp.counter + bp.counter_sel, 1);
         __syncthreads();
         const int b = tile_id;
-        if (b >= total) return;
+        if (b >= total) {
+            if (tid == 0 && cur >= 0 && bp.mode[cur] == 0 && sa.field_amax != nullptr && s_blk_amax != 0u)
+                atomicMax(sa.field_amax, s_blk_amax);
+            return;
+        }
         int s = 0;
         while (s + 1 < bp.nslots && b >= bp.first[s + 1]) ++s;
         if (s != cur) {  // every thread takes the same branch
+            if (tid == 0 && cur >= 0 && bp.mode[cur] == 0 && sa.field_amax != nullptr && s_blk_amax != 0u)
+                atomicMax(sa.field_amax, s_blk_amax);
+            __syncthreads();  // the flush reads sa before it is replaced
+            if (tid == 0) s_blk_amax = 0u;
             const long long* src = reinterpret_cast<const long long*>(bp.args[s]);
             long long* dst = reinterpret_cast<long long*>(&sa);
             for (int i = tid; i < kWords; i += NT) dst[i] = src[i];
@@ -749,7 +887,9 @@ __global__ void __launch_bounds__(NT) batch_step_kernel(const BatchParams bp) {
             cur = s;
         }
         const int lb = b - bp.first[s];
-        const bool ok = bp.mode[s] == 0 ? run_tile<0>(sa, sm, &bar, phase, lb) : run_tile<1>(sa, sm, &bar, phase, lb);
+        const int md = bp.mode[s];
+        const bool ok = md == 0 ? run_tile<0>(sa, sm, &bar, phase, lb)
+                                : (md == 1 ? run_tile<1>(sa, sm, &bar, phase, lb) : run_tile<2>(sa, sm, &bar, phase, lb));
         if (!ok) return;
         __syncthreads();  // shared tile, tile_id and (next switch) sa are reused
     }
@@ -894,13 +1034,29 @@ int launch_mode(const StepArgs& a, cudaStream_t stream) {
 int prepare_step_kernels() {
     // Kernel attributes and occupancy are set up once, outside any stream
     // capture.
-    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && batch_blocks_per_sm() > 0) ? (int)cudaGetLastError()
-                                                                                            : 1;
+    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && blocks_per_sm<2>() > 0 && batch_blocks_per_sm() > 0)
+               ? (int)cudaGetLastError()
+               : 1;
 }
 
 int launch_step(int mode, const StepArgs& a, void* stream) {
     if (a.r_first[a.nrect] <= 0) return 0;
-    return mode == 0 ? launch_mode<0>(a, (cudaStream_t)stream) : launch_mode<1>(a, (cudaStream_t)stream);
+    if (mode == 0) return launch_mode<0>(a, (cudaStream_t)stream);
+    if (mode == 1) return launch_mode<1>(a, (cudaStream_t)stream);
+    return launch_mode<2>(a, (cudaStream_t)stream);
+}
+
+__global__ void quantize_kernel(const float* src, const unsigned int* amax, void* dst, float* iscale, int n,
+                                int kind16) {
+    quantize_part(src, amax, dst, iscale, n, kind16, threadIdx.y * 32 + threadIdx.x);
+}
+
+int launch_quantize(const float* src, const unsigned int* amax, void* dst, float* iscale, int n, int kind16,
+                    void* stream) {
+    if (n <= 0) return 0;
+    const int blocks = min((n / 4 + NT - 1) / NT, 148 * 8);
+    quantize_kernel<<<blocks, dim3(32, NWARP), 0, (cudaStream_t)stream>>>(src, amax, dst, iscale, n, kind16);
+    return (int)cudaGetLastError();
 }
 
 int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
