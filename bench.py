@@ -224,6 +224,57 @@ def run_reference(args):
 
 # ---- GPU arm -----------------------------------------------------------------
 
+# The engine's other forms, timed after the drop-in on the same shots:
+# (name, precision, store_snap, slots); slots = 0 is one shot at a time
+# through psdm_rtm_shot_device, otherwise psdm_rtm_batch_device with that
+# many shots in flight.  precision 1 / 2 = binary16 / bfloat16 snapshots.
+FORMS = [
+    ("fp16_ks4", 1, 4, 0),
+    ("batch_fp16_ks4", 1, 4, 8),
+    ("batch_bf16_ks4", 2, 4, 8),
+    ("batch_fp32", 0, 1, 2),
+]
+
+
+def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
+    """Shots/s of each named form on the workload's shots (inputs in HBM)."""
+    from psdm_b200 import rtm
+    out = {}
+    outs = [torch.zeros((it["nx_w"], NY), dtype=torch.float32, device=dev) for it in items]
+    for name, precision, ks, slots in FORMS:
+        if name not in names:
+            continue
+        prm = rtm.Params(dPML=DPML, fs=1, strategy=1, precision=precision)
+        n = 2 * slots if slots else 4
+        sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
+
+        def run(k):
+            if slots == 0:
+                for it, o in sel[:k]:
+                    engine.rtm_shot_device(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], d_src.data_ptr(),
+                                           it["d_obs"].data_ptr(), DD, DT, NY, NX, it["nx_w"], it["d_vp"].data_ptr(),
+                                           ADDED_SPACE, ks, NT, NT, NT, 0, 1, 0, o.data_ptr())
+            else:
+                descs = [dict(nxSou=it["nxSou"], nySou=it["nySou"], nxRec=it["nxRec"], nyRec=it["nyRec"],
+                              nx_w=it["nx_w"], nt_prop2=NT, nt_taper=NT, d_Vp_w=it["d_vp"].data_ptr(),
+                              d_Data_target=it["d_obs"].data_ptr(), d_PSDM_w=o.data_ptr()) for it, o in sel[:k]]
+                engine.rtm_batch_device(prm, descs, d_src.data_ptr(), DD, DT, NY, NX, ADDED_SPACE, store_snap=ks,
+                                        max_slots=slots)
+
+        run(max(slots, 1))  # warm-up: buffers, graphs
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(n)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        v = n / (e0.elapsed_time(e1) / 1e3)
+        out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
+                     "slots": engine.batch_slots() if slots else 1, "precision": ["f32", "fp16", "bf16"][precision],
+                     "store_snap": ks}
+    return out
+
+
 def build_inputs(engine, torch, dev, shots, survey, vel_true, vel_mig, prm):
     """Device-resident inputs of each shot (model window, source, observed data)."""
     from psdm_b200 import rtm, synth
@@ -352,6 +403,11 @@ def run_gpu(args):
         e2e = {"value": world * args.steps / float(el.item()), "unit": "shots/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "api": "psdm_rtm_shot (C ABI, pinned host buffers)"}
 
+    forms = None
+    names = [f[0] for f in FORMS] if args.forms == "all" else [n for n in args.forms.split(",") if n and n != "none"]
+    if world == 1 and names:
+        forms = time_forms(engine, torch, dev, stream, d_src, items_u, names, value)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_sample(cpu_procs(32), 12)
@@ -378,6 +434,7 @@ def run_gpu(args):
                 "gpu_launches": int(st["launches"]),
                 "clocks": clk.summary(),
                 "e2e": e2e,
+                "forms": forms,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -392,6 +449,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--forms", default="all",
+                    help="other engine forms to time after the drop-in: all, none or a comma list of " +
+                         ", ".join(f[0] for f in FORMS))
     ap.add_argument("--nt", type=int, default=None,
                     help="override the record length (small cases for ncu captures only; not a bench value)")
     args = ap.parse_args()

@@ -411,21 +411,14 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     const int sz0 = z0 - 4, sx0 = x0 - 3;
     const int dn = a.dn;
     float* ps = sm;                  // p, (ncols+6) columns of HZ rows
-    float* pms = ps + WX * HZ;       // p1, ncols columns of TZ rows
-    float* c2s = pms + TX * TZ;      // c2
     if (wy == 0) {
-        const uint32_t prow = (uint32_t)(nrows + 8) * 4u, trow = (uint32_t)nrows * 4u;
-        const uint32_t bytes = (uint32_t)(ncols + 6) * prow + (uint32_t)ncols * trow * 2u;
+        const uint32_t prow = (uint32_t)(nrows + 8) * 4u;
+        const uint32_t bytes = (uint32_t)(ncols + 6) * prow;
         fence_proxy_async();  // the previous tile's shared reads precede these writes
         if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
         __syncwarp();
         for (int c = lane; c < ncols + 6; c += 32)
             bulk_g2s(ps + c * HZ, a.p + (sx0 + c) * a.ldz + sz0, prow, bar);
-        for (int c = lane; c < ncols; c += 32) {
-            const int g = (x0 + c) * a.ldz + z0;
-            bulk_g2s(pms + c * TZ, a.pm + g, trow, bar);
-            bulk_g2s(c2s + c * TZ, a.c2 + g, trow, bar);
-        }
     }
     const int q = 4 * lane;        // first tile row of this thread's float4
     const int c0 = wy * XS;        // first tile column of this thread
@@ -447,6 +440,15 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         Cn = *reinterpret_cast<const float4*>(a.comp + fi);
     }
     float amax_t = 0.f;
+    // p1 and c2 of the first column, from global memory while p lands; later
+    // columns are fetched one column ahead.
+    float* __restrict__ pmp = a.pm;
+    int g = (x0 + c0) * a.ldz + zd;
+    float4 pmN = make_float4(0.f, 0.f, 0.f, 0.f), c2N = pmN;
+    if (active) {
+        pmN = *reinterpret_cast<const float4*>(pmp + g);
+        c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
+    }
     const bool ok = mbar_wait_bounded(bar, phase);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -460,8 +462,6 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     float4 win[7];
 #pragma unroll
     for (int k = 0; k < 6; ++k) win[k] = ps4[(c0 + k) * HQ + qr];
-    float* __restrict__ pmp = a.pm;
-    int g = (x0 + c0) * a.ldz + zd;
     float2 cc[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) cc[k] = make_float2(a.cf2[k], a.cf2[k]);
@@ -473,8 +473,11 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         win[6] = ps4[(col + 6) * HQ + qr];
         const float4 zm = ps4[(col + 3) * HQ + qr - 1];
         const float4 zp = ps4[(col + 3) * HQ + qr + 1];
-        const float4 pmv = *reinterpret_cast<const float4*>(pms + col * TZ + q);
-        const float4 c2v = *reinterpret_cast<const float4*>(c2s + col * TZ + q);
+        const float4 pmv = pmN, c2v = c2N;
+        if (c + 1 < ncol) {
+            pmN = *reinterpret_cast<const float4*>(pmp + g + a.ldz);
+            c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g + a.ldz));
+        }
         float4 Fc = Fn, Ic = In, Cc = Cn;
         if (img && c + 1 < ncol) {  // next column of the snapshot and image
             Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi + a.ldf));
@@ -758,11 +761,11 @@ __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r
 
 template <int MODE>
 constexpr int smem_floats() {
-    return WX * HZ + TX * TZ * 2;
+    return WX * HZ;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(NT) step_kernel(const StepArgs a) {
+__global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_id;
@@ -831,7 +834,7 @@ __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t*
 // step of many shots fills the GPU in several waves.  Each slot's step
 // arguments live in device memory; a block copies them into shared memory
 // when it switches slot.  Slots may be in different passes (mode 0 / 1).
-__global__ void __launch_bounds__(NT) batch_step_kernel(const BatchParams bp) {
+__global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_id;
