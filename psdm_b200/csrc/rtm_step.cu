@@ -76,6 +76,8 @@ constexpr int ZTX = NWARP * ZXS;
 constexpr int ZWX = ZTX + 6;
 constexpr int RTX = 64;
 constexpr int NT = 32 * NWARP;  // threads per block
+// C-PML strip tiles also stage their phi tile, after the p tile.
+constexpr int PHI_OFF = WX * HZ;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -117,6 +119,25 @@ __device__ __forceinline__ float div_dt(const StepArgs& a, float x) {
     }
     return q;
 }
+
+// x / dt for the common inputs -- x = +-0 (kept with its sign) or |x| in
+// [div_lo, div_hi] with the fast form enabled -- without branches; `rare`
+// is set for any other input, which div_dt then handles.
+__device__ __forceinline__ float div_dt_common(const StepArgs& a, float x, bool& rare) {
+    const float ax = fabsf(x);
+    const float q0 = __fmul_rn(x, a.inv_dt);
+    const float e = __fmaf_rn(-q0, a.dt, x);
+    const float q1 = __fmaf_rn(e, a.inv_dt, q0);
+    rare = rare || !(ax == 0.f || (a.fast_div && ax >= a.div_lo && ax <= a.div_hi));
+    return ax == 0.f ? x : q1;
+}
+
+// Programmatic dependent launch: a step is launched with programmatic
+// stream serialization, so its launch is processed while the previous step
+// finishes; it touches nothing before the previous launch has completed and
+// its writes are visible.  (Triggering the dependent launch early made the
+// single-shot step slower: the waiting blocks take resident slots.)
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ float comp(const float4& v, int r) {
     return r == 0 ? v.x : (r == 1 ? v.y : (r == 2 ? v.z : v.w));
@@ -240,15 +261,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // Stage rows [sz0, sz0+4*hq) x columns [sx0, sx0+wx) of p in shared memory
 // (zero outside the array).  sz0 is a multiple of 4.
-__device__ __forceinline__ void load_tile(const StepArgs& a, float* ps, int sz0, int sx0, int hq, int wx, int tid) {
+__device__ __forceinline__ void load_tile_from(const float* src, const StepArgs& a, float* ps, int sz0, int sx0, int hq,
+                                               int wx, int tid) {
     for (int q = tid; q < wx * hq; q += NT) {
         const int col = q / hq, r4 = q - col * hq;
         const int gx = sx0 + col, gz = sz0 + 4 * r4;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (gx >= 0 && gx < a.nxt && gz >= 0 && gz < a.ldz)
-            v = __ldg(reinterpret_cast<const float4*>(a.p + gx * a.ldz + gz));
+            v = __ldg(reinterpret_cast<const float4*>(src + gx * a.ldz + gz));
         *reinterpret_cast<float4*>(&ps[col * (4 * hq) + 4 * r4]) = v;
     }
+}
+__device__ __forceinline__ void load_tile(const StepArgs& a, float* ps, int sz0, int sx0, int hq, int wx, int tid) {
+    load_tile_from(a.p, a, ps, sz0, sx0, hq, wx, tid);
 }
 
 // Any cell of the grid: C-PML strips and corners, free-surface row,
@@ -519,11 +544,22 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         const float4 out = make_float4(oA.x, oA.y, oB.x, oB.y);
         *reinterpret_cast<float4*>(pmp + g) = out;
         if (MODE == 0 && a.field != nullptr) {
+            const float hx = __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f);
+            const float hy = __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f);
+            const float hz = __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f);
+            const float hw = __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f);
+            bool rare = false;
             float4 sv;
-            sv.x = div_dt(a, __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f));
-            sv.y = div_dt(a, __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f));
-            sv.z = div_dt(a, __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f));
-            sv.w = div_dt(a, __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f));
+            sv.x = div_dt_common(a, hx, rare);
+            sv.y = div_dt_common(a, hy, rare);
+            sv.z = div_dt_common(a, hz, rare);
+            sv.w = div_dt_common(a, hw, rare);
+            if (__any_sync(__activemask(), rare) && rare) {
+                sv.x = div_dt(a, hx);
+                sv.y = div_dt(a, hy);
+                sv.z = div_dt(a, hz);
+                sv.w = div_dt(a, hw);
+            }
             *reinterpret_cast<float4*>(a.field + fi) = sv;
             if (a.field_amax != nullptr)
                 amax_t = fmaxf(amax_t, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(sv.z), fabsf(sv.w))));
@@ -603,6 +639,10 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     const int sz0 = z0 - 4;
     const int sx0 = min(x0, a.nxt - 4) - 3;
     load_tile(a, ps, sz0, sx0, HQ, PWX, tid);
+    // phi columns: x0-6 .. x0+21 covers ci-3 .. ci+3 for every column of the
+    // tile, ci being clamped into the strip.
+    const int sxp = x0 - 6;
+    load_tile_from(a.phix_in, a, ps + PHI_OFF, sz0, sxp, HQ, PTX + 12, tid);
     __syncthreads();
     const int zd = z0 + 4 * lane;
     if (zd >= zend) return;
@@ -610,6 +650,7 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     const int z = zd - a.zoff;
     const bool fsq = a.fs && z == dn;
     const float4* __restrict__ ps4 = reinterpret_cast<const float4*>(ps);
+    const float4* __restrict__ ph4 = reinterpret_cast<const float4*>(ps + PHI_OFF);
     const int qr = (zd - sz0) >> 2;
     const float* c1 = a.cf1;
     const float* c2 = a.cf2;
@@ -632,9 +673,9 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
         float4 F[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k)
-            if (k != 3) F[k] = __ldg(reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd));
+            if (k != 3) F[k] = ph4[(ci + k - 3 - sxp) * HQ + qr];
         F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 phc = __ldg(reinterpret_cast<const float4*>(a.phix_in + g));
+        const float4 phc = ph4[(x - sxp) * HQ + qr];
         const float4 chc = *reinterpret_cast<const float4*>(a.chix + g);
         const float4 pmv = *reinterpret_cast<const float4*>(a.pm + g);
         const float4 c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
@@ -683,6 +724,9 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     const int sz0 = (min(z0, nr - 4) - 3) & ~3;
     const int sx0 = x0 - 3;  // interior columns: no clamping along x
     load_tile(a, ps, sz0, sx0, PHQ, ZWX, tid);
+    // phi rows: 4 more above the p tile, so that cj-3 stays inside when a
+    // tile starts within 3 rows of a strip's end.
+    load_tile_from(a.phiz_in, a, ps + PHI_OFF, sz0 - 4, sx0, PHQ + 1, ZWX, tid);
     __syncthreads();
     const int zd = z0 + lane;
     if (zd >= zend) return;
@@ -720,12 +764,12 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
         const float d1 = D1(AZ, c1);
 #undef AX
         const int g = x * a.ldz + zd;
-        const float* ph = a.phiz_in + x * a.ldz + cj;
-#define PZ(k) __ldg(ph + (k))
+        const float* phs = ps + PHI_OFF + xl * (PHZ + 4) + 4 - sz0;
+#define PZ(k) phs[cj + (k)]
         const float dph = D1(PZ, c1);
 #undef PZ
 #undef AZ
-        const float phn = __fadd_rn(__fmul_rn(A, __ldg(a.phiz_in + g)), __fmul_rn(B, d1));
+        const float phn = __fadd_rn(__fmul_rn(A, phs[zd]), __fmul_rn(B, d1));
         const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
         a.phiz_out[g] = phn;
         a.chiz[g] = chn;
@@ -761,7 +805,7 @@ __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r
 
 template <int MODE>
 constexpr int smem_floats() {
-    return WX * HZ;
+    return PHI_OFF + HZ * (PTX + 12);  // p tile; phi tile of the C-PML strip tiles
 }
 
 template <int MODE>
@@ -770,6 +814,7 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
     __shared__ __align__(8) uint64_t bar;
     __shared__ int tile_id;
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    grid_dependency_wait();
     if (tid == 0) {
         mbar_init(&bar, 1);
         s_blk_amax = 0u;
@@ -840,6 +885,7 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
     __shared__ int tile_id;
     __shared__ __align__(16) StepArgs sa;
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    grid_dependency_wait();
     if (tid == 0) {
         mbar_init(&bar, 1);
         s_blk_amax = 0u;
@@ -1030,8 +1076,17 @@ template <int MODE>
 int launch_mode(const StepArgs& a, cudaStream_t stream) {
     const int bytes = smem_floats<MODE>() * (int)sizeof(float);
     const dim3 grid(min(a.r_first[a.nrect], a.num_sms * blocks_per_sm<MODE>()));
-    step_kernel<MODE><<<grid, dim3(32, NWARP), bytes, stream>>>(a);
-    return (int)cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(32, NWARP);
+    cfg.dynamicSmemBytes = (size_t)bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, step_kernel<MODE>, a);
 }
 
 int prepare_step_kernels() {
@@ -1067,8 +1122,17 @@ int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
     if (bp.nslots <= 0 || total <= 0) return 0;
     const int bytes = smem_floats<0>() * (int)sizeof(float);
     const dim3 grid(min(total, num_sms * batch_blocks_per_sm()));
-    batch_step_kernel<<<grid, dim3(32, NWARP), bytes, (cudaStream_t)stream>>>(bp);
-    return (int)cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(32, NWARP);
+    cfg.dynamicSmemBytes = (size_t)bytes;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, batch_step_kernel, bp);
 }
 
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream) {
