@@ -190,6 +190,15 @@ int psdm_rtm_batch_device(
 int32_t psdm_engine_batch_slots(const psdm_engine* e);
 
 /*
+ * Exercise the engine's failure path without a GPU fault (no reference
+ * counterpart): one kernel waits, with the step kernels' time limit (about
+ * 1 s), for copies that are never issued, gives up and reports through the
+ * engine's error word.  Returns PSDM_ERR_CUDA with the step kernels' timeout
+ * message when the path works; the engine stays usable afterwards.
+ */
+int psdm_engine_check_wait_timeout(psdm_engine* e);
+
+/*
  * Forward modelling only (the receiver output Rec_point of
  * solver_ac_forward_ram, src/solver_ac_forward_ram.f90:567-577) without
  * storing snapshots: synthetic shot gathers for least-squares or QC.

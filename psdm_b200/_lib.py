@@ -23,6 +23,7 @@ EXPORTS = [
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
     "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
+    "psdm_engine_check_wait_timeout",
 ]
 
 
@@ -90,6 +91,7 @@ def lib():
     L.psdm_rtm_batch_device.argtypes = [_P, PP, _I, C.POINTER(Shot), _P, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]
     L.psdm_engine_batch_slots.argtypes = [_P]
     L.psdm_engine_batch_slots.restype = _I
+    L.psdm_engine_check_wait_timeout.argtypes = [_P]
     L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
     L.psdm_fd_coef.restype = None
     L.psdm_pml_coeffs.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _P]

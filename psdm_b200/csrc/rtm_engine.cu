@@ -1339,6 +1339,14 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
 
 int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
 
+int psdm_engine_check_wait_timeout(psdm_engine* e) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    const int rc = launch_wait_timeout_probe(e->d_err, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "probe launch: %s", cudaGetErrorString((cudaError_t)rc));
+    return sync(e);
+}
+
 int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
                     const int32_t* nxRec, const int32_t* nyRec, const float* Data_source, float dd, float dt,
                     int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w, float dd_space, int32_t nt,

@@ -137,6 +137,8 @@ int launch_step(int mode, const StepArgs& a, void* stream);
 // Quantize one snapshot outside a step launch (see StepArgs::q_*).
 int launch_quantize(const float* src, const unsigned int* amax, void* dst, float* iscale, int n, int kind16,
                     void* stream);
+// One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
+int launch_wait_timeout_probe(int* err, void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.
 int launch_batch_step(const BatchParams& bp, int num_sms, void* stream);
 // Receiver gather after the last forward step (Rec(nt-1) and Rec(nt)).

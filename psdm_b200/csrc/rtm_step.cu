@@ -1135,6 +1135,23 @@ int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
     return (int)cudaLaunchKernelEx(&cfg, batch_step_kernel, bp);
 }
 
+// A bounded wait on copies that are never issued: the mbarrier expects 16
+// bytes that no copy delivers, so the wait gives up after its time limit and
+// reports through `err` exactly as a step kernel does.  Nothing is in flight,
+// so returning is safe.
+__global__ void wait_timeout_probe_kernel(int* err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, 16u);
+    if (!mbar_wait_bounded(&bar, 0u)) atomicExch(err, 1);
+}
+
+int launch_wait_timeout_probe(int* err, void* stream) {
+    wait_timeout_probe_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(err);
+    return (int)cudaGetLastError();
+}
+
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream) {
     if (nrec <= 0 || nt < 2) return 0;
     rec_final_kernel<<<(nrec + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rec_cell, p, rec_out, nrec, rec_ld, nt);

@@ -193,6 +193,10 @@ class Engine:
                                               dt, ny, nx, added_space, store_snap, taper_option, N_taper, N_zeros,
                                               max_slots))
 
+    def check_wait_timeout(self):
+        """psdm_engine_check_wait_timeout: raises PsdmError when the failure path works."""
+        L.check(L.lib().psdm_engine_check_wait_timeout(self._h))
+
     def batch_slots(self) -> int:
         return int(L.lib().psdm_engine_batch_slots(self._h))
 
