@@ -264,6 +264,50 @@ void psdm_taper_pad_trace(float* trace, int32_t nt_prop, int32_t N_taper, int32_
 void psdm_optimization_dt(float dmodel_prop, float vmax, float tfin, int32_t store_snap,
                           float* dt_prop, int32_t* nt_prop, int32_t* nt_snap);
 
+/* ---- trace conditioning (src/calculate_PSDM_RTM.f90:231-355) ---------------- */
+
+/* Parfile switches of the conditioning (modules.f90: cut_multiple, cut_sf,
+ * taper_option, T_taper, T_zeros; T_taper after the reader's default rule
+ * T_taper = T_zeros/4 when it is 0, modules.f90:556). */
+typedef struct psdm_conditioning {
+    int32_t cut_multiple;
+    int32_t cut_sf;
+    int32_t taper_option;
+    float T_taper, T_zeros; /* seconds */
+} psdm_conditioning;
+
+/*
+ * Time windows of one shot (calculate_PSDM_RTM.f90:231-291), the reference's
+ * FP32 arithmetic: per trace nt_cut (before the sea-floor multiple) and nt_sf
+ * (after the direct water wave), from the sea-floor depth Batmodel (nx_prop
+ * values, metres) at the source-receiver midpoint; then lens = {nt_prop2,
+ * nt_taper, N_taper, N_zeros}.
+ */
+void psdm_trace_windows(const psdm_conditioning* c, int32_t NumRec, int32_t nxSou, int32_t nySou,
+                        const int32_t* nxRec, const int32_t* nyRec, const float* Batmodel,
+                        float dmodel_prop, float dt_prop, int32_t nt_prop, int32_t* nt_cut,
+                        int32_t* nt_sf, int32_t* lens /* 4 */);
+
+/*
+ * Data_target (nt_taper, NumRec) from Field_Data (nt_data, NumRec) on the GPU
+ * (calculate_PSDM_RTM.f90:316-355): resampling from dt_data to dt_prop by
+ * Akima's local cubic interpolation when they differ (in place of the
+ * reference's vendored TOMS-433 routine, interpolation_akima.f90), the
+ * sea-floor cut, the multiple cut and the taper with zero padding.  The
+ * frequency filter (freq_filter) is not part of it: filter Field_Data first.
+ * nt_cut, nt_sf and lens come from psdm_trace_windows.
+ */
+int psdm_condition_traces(psdm_engine* e, const psdm_conditioning* c, int32_t NumRec,
+                          const float* Field_Data, int32_t nt_data, float dt_data, float dt_prop,
+                          const int32_t* nt_cut, const int32_t* nt_sf, const int32_t* lens,
+                          float* Data_target);
+/* Same with device pointers for Field_Data and Data_target (nt_cut, nt_sf and
+ * lens stay on the host); asynchronous on the engine's stream. */
+int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int32_t NumRec,
+                                 const float* d_Field_Data, int32_t nt_data, float dt_data,
+                                 float dt_prop, const int32_t* nt_cut, const int32_t* nt_sf,
+                                 const int32_t* lens, float* d_Data_target);
+
 /* normalize_psdm (src/auxiliar_PSDM.f90:1-20): PSDM = sum/fold where fold > 0. */
 void psdm_normalize_psdm(int32_t nx, int32_t ny, const float* PSDM_sum, const float* Cov_sum,
                          float* PSDM);

@@ -67,6 +67,10 @@ def lib():
                       _I, _I, _I, _I, _I, _I]
         L.orc_rtm_shot_mixed_f.argtypes = [_I, _I] + mixed_args + [_f32p, C.c_void_p]
         L.orc_rtm_shot_mixed_d.argtypes = mixed_args + [_f64p, C.c_void_p]
+        L.orc_trace_windows.argtypes = [_I, _I, _I, _F, _F, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _i32p,
+                                        _i32p, _i32p]
+        L.orc_akima.argtypes = [_f32p, _I, _F, _I, _F, _f32p]
+        L.orc_condition_traces.argtypes = [_I, _I, _I, _I, _f32p, _I, _F, _F, _I, _I, _I, _I, _i32p, _i32p, _f32p]
         _lib = L
     return _lib
 
@@ -204,6 +208,38 @@ def rtm_shot_mixed(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, 
     else:
         lib().orc_rtm_shot_mixed_d(*args)
     return (img, F[:nsnap]) if want_fields else img
+
+
+def trace_windows(*, cut_multiple, cut_sf, taper_option, T_taper, T_zeros, nxSou, nySou, nxRec, nyRec, Batmodel,
+                  dmodel_prop, dt_prop, nt_prop):
+    """calculate_PSDM_RTM.f90:231-291: (nt_cut, nt_sf, nt_prop2, nt_taper, N_taper, N_zeros)."""
+    nxRec = _i32(nxRec)
+    n = nxRec.size
+    nt_cut = np.zeros(n, np.int32)
+    nt_sf = np.zeros(n, np.int32)
+    out = np.zeros(4, np.int32)
+    lib().orc_trace_windows(cut_multiple, cut_sf, taper_option, T_taper, T_zeros, n, int(nxSou), int(nySou), nxRec,
+                            _i32(nyRec), _f32(Batmodel), dmodel_prop, dt_prop, nt_prop, nt_cut, nt_sf, out)
+    return nt_cut, nt_sf, int(out[0]), int(out[1]), int(out[2]), int(out[3])
+
+
+def akima(y, dx: float, m: int, dt: float) -> np.ndarray:
+    """Akima interpolation of y (x_k = k*dx) at t_i = i*dt, i < m."""
+    y = _f32(y).reshape(-1)
+    out = np.zeros(m, np.float32)
+    lib().orc_akima(y, y.size, dx, m, dt, out)
+    return out
+
+
+def condition_traces(*, cut_multiple, cut_sf, taper_option, Field_Data, dt_data, dt_prop, nt_prop2, nt_taper,
+                     N_taper, N_zeros, nt_cut, nt_sf) -> np.ndarray:
+    """calculate_PSDM_RTM.f90:316-355 (no frequency filter): Data_target as (NumRec, nt_taper)."""
+    F = _f32(Field_Data)
+    nrec, nt_data = F.shape
+    out = np.zeros((nrec, nt_taper), np.float32)
+    lib().orc_condition_traces(cut_multiple, cut_sf, taper_option, nrec, F.reshape(-1), nt_data, dt_data, dt_prop,
+                               nt_prop2, nt_taper, N_taper, N_zeros, _i32(nt_cut), _i32(nt_sf), out)
+    return out
 
 
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:

@@ -831,3 +831,146 @@ void orc_normalize_psdm(int nx, int ny, const float* PSDM_sum, const float* Cov_
 }
 
 }  // extern "C"
+
+// ---- trace conditioning (src/calculate_PSDM_RTM.f90:231-355) ----------------
+//
+// The per-shot preparation of the observed data before the backward pass:
+// travel-time windows from the bathymetry, resampling to the propagation
+// time step, the sea-floor cut, the multiple cut and the taper.  The
+// frequency filter (freq_filter, auxiliar.f90:498-531) is not restated.
+
+namespace {
+
+// Time-window lengths (calculate_PSDM_RTM.f90:231-291), FP32 as the
+// reference: nt_cut / nt_sf per trace, then nt_prop2, nt_taper, N_taper,
+// N_zeros.  Batmodel is indexed with the 1-based model column mid_x.
+void trace_windows(int cut_multiple, int cut_sf, int taper_option, float T_taper, float T_zeros, int NumRec,
+                   int nxSou, int nySou, const int* nxRec, const int* nyRec, const float* Batmodel,
+                   float dmodel_prop, float dt_prop, int nt_prop, int* nt_cut, int* nt_sf, int* nt_prop2,
+                   int* nt_taper, int* N_taper, int* N_zeros) {
+    for (int j = 0; j < NumRec; ++j) {
+        nt_cut[j] = nt_prop;  // :123
+        nt_sf[j] = 1;         // :124
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        if ((pass == 0 && cut_multiple <= 0) || (pass == 1 && cut_sf <= 0)) continue;
+        for (int j = 0; j < NumRec; ++j) {
+            const float offset = std::fabs(float(nxSou) * dmodel_prop - float(nxRec[j]) * dmodel_prop);
+            const int mid_x = (int)std::ceil(0.5f * float(nxSou + nxRec[j]));
+            const float D_src = Batmodel[mid_x - 1] - float(nySou) * dmodel_prop;
+            const float D_rec = Batmodel[mid_x - 1] - float(nyRec[j]) * dmodel_prop;
+            const float a = offset * 0.5f, b = 0.5f * (D_src + D_rec);
+            const float leg = std::sqrt(a * a + b * b);
+            if (pass == 0) {
+                const float twt = (4.0f * leg) / 1500.f;
+                nt_cut[j] = (int)std::ceil((0.9f * twt) / dt_prop);
+            } else {
+                const float twt = (2.0f * leg) / 1500.f;
+                nt_sf[j] = (int)std::ceil((1.1f * twt) / dt_prop);
+            }
+        }
+    }
+    *nt_prop2 = nt_prop;
+    *nt_taper = nt_prop;
+    *N_taper = 1;
+    *N_zeros = 0;
+    if (taper_option != 0 || cut_multiple != 0) {
+        *N_taper = std::max(1, (int)(T_taper / dt_prop));
+        *N_zeros = std::max(0, (int)(T_zeros / dt_prop));
+        int mx = nt_cut[0];
+        for (int j = 1; j < NumRec; ++j) mx = std::max(mx, nt_cut[j]);
+        *nt_prop2 = std::min(nt_prop, mx);
+        *nt_taper = *nt_prop2 + *N_zeros;
+    }
+}
+
+// Akima's (1970) local cubic interpolation of y sampled at x_k = k*dx
+// (k = 0..n-1), evaluated at t; the end slopes are extended with
+// m[-1] = 2m[0] - m[1], m[-2] = 2m[-1] - m[0] (and mirrored at the far end),
+// and points outside the data use the end interval's cubic.  Written from
+// the published method; the engine's kernel evaluates the same expressions
+// in the same order.
+struct AkimaTrace {
+    const float* y;
+    int n;
+    float dx;
+    float x(int k) const { return float(k) * dx; }
+    float m(int k) const {  // slope of interval k, extended beyond both ends
+        if (k < 0) {
+            const float m0 = m(0), m1 = m(1);
+            const float mm1 = 2.f * m0 - m1;
+            return k == -1 ? mm1 : 2.f * mm1 - m0;
+        }
+        if (k > n - 2) {
+            const float a = m(n - 2), b = m(n - 3);
+            const float mp = 2.f * a - b;
+            return k == n - 1 ? mp : 2.f * mp - a;
+        }
+        return (y[k + 1] - y[k]) / (x(k + 1) - x(k));
+    }
+    float slope_at(int k) const {  // derivative at point k
+        const float w1 = std::fabs(m(k + 1) - m(k)), w2 = std::fabs(m(k - 1) - m(k - 2));
+        if (w1 + w2 == 0.f) return 0.5f * (m(k - 1) + m(k));
+        return (w1 * m(k - 1) + w2 * m(k)) / (w1 + w2);
+    }
+    float at(float t) const {
+        if (n == 1) return y[0];
+        if (n == 2) return y[0] + (t - x(0)) * ((y[1] - y[0]) / (x(1) - x(0)));
+        if (t == x(n - 1)) return y[n - 1];
+        int j = (int)(t / dx);
+        j = std::min(std::max(j, 0), n - 2);
+        while (j > 0 && t < x(j)) --j;
+        while (j < n - 2 && t >= x(j + 1)) ++j;
+        const float h = x(j + 1) - x(j), d = t - x(j);
+        const float tj = slope_at(j), tj1 = slope_at(j + 1), mj = m(j);
+        const float p2 = (3.f * mj - 2.f * tj - tj1) / h;
+        const float p3 = (tj + tj1 - 2.f * mj) / (h * h);
+        return y[j] + d * (tj + d * (p2 + d * p3));
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+void orc_trace_windows(int cut_multiple, int cut_sf, int taper_option, float T_taper, float T_zeros, int NumRec,
+                       int nxSou, int nySou, const int* nxRec, const int* nyRec, const float* Batmodel,
+                       float dmodel_prop, float dt_prop, int nt_prop, int* nt_cut, int* nt_sf, int* out4) {
+    trace_windows(cut_multiple, cut_sf, taper_option, T_taper, T_zeros, NumRec, nxSou, nySou, nxRec, nyRec, Batmodel,
+                  dmodel_prop, dt_prop, nt_prop, nt_cut, nt_sf, out4, out4 + 1, out4 + 2, out4 + 3);
+}
+
+void orc_akima(const float* y, int n, float dx, int m, float dt, float* out) {
+    AkimaTrace a{y, n, dx};
+    for (int i = 0; i < m; ++i) out[i] = a.at(float(i) * dt);
+}
+
+// Data_target (nt_taper, NumRec) from Field_Data (nt_data, NumRec),
+// calculate_PSDM_RTM.f90:316-355 without the frequency filter.
+void orc_condition_traces(int cut_multiple, int cut_sf, int taper_option, int NumRec, const float* Field_Data,
+                          int nt_data, float dt_data, float dt_prop, int nt_prop2, int nt_taper, int N_taper,
+                          int N_zeros, const int* nt_cut, const int* nt_sf, float* Data_target) {
+    for (int i = 0; i < NumRec; ++i) {
+        float* tr = Data_target + (size_t)i * nt_taper;
+        const float* f = Field_Data + (size_t)i * nt_data;
+        for (int s = 0; s < nt_taper; ++s) tr[s] = 0.f;
+        if (dt_data != dt_prop) {
+            AkimaTrace a{f, nt_data, dt_data};
+            for (int s = 0; s < nt_prop2; ++s) tr[s] = a.at(float(s) * dt_prop);
+        } else {
+            for (int s = 0; s < nt_prop2 && s < nt_data; ++s) tr[s] = f[s];
+        }
+        if (cut_sf > 0)
+            for (int s = 0; s < nt_sf[i] && s < nt_taper; ++s) tr[s] = 0.f;
+        if (cut_multiple == 0) {
+            if (taper_option != 0) taper_pad_trace<float>(tr, nt_prop2, N_taper, N_zeros, nt_taper);
+        } else {
+            // guard: the reference indexes outside the trace if nt_cut > nt_taper or < 1
+            const int c = std::max(1, std::min(nt_cut[i], nt_taper));
+            for (int s = c - 1; s < nt_taper; ++s) tr[s] = 0.f;
+            taper_pad_trace<float>(tr, c, N_taper, N_zeros, nt_taper);
+        }
+    }
+}
+
+}  // extern "C"

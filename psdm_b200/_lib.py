@@ -23,7 +23,7 @@ EXPORTS = [
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
     "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
-    "psdm_engine_check_wait_timeout",
+    "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
 ]
 
 
@@ -41,6 +41,12 @@ class Shot(C.Structure):
     _fields_ = [("NumRec", C.c_int32), ("nxSou", C.c_int32), ("nySou", C.c_int32), ("nxRec", C.c_void_p),
                 ("nyRec", C.c_void_p), ("nx_w", C.c_int32), ("nt_prop2", C.c_int32), ("nt_taper", C.c_int32),
                 ("Vp_w", C.c_void_p), ("Data_target", C.c_void_p), ("PSDM_w", C.c_void_p)]
+
+
+class Conditioning(C.Structure):
+    """struct psdm_conditioning."""
+    _fields_ = [("cut_multiple", C.c_int32), ("cut_sf", C.c_int32), ("taper_option", C.c_int32),
+                ("T_taper", C.c_float), ("T_zeros", C.c_float)]
 
 
 class PsdmError(RuntimeError):
@@ -92,6 +98,11 @@ def lib():
     L.psdm_engine_batch_slots.argtypes = [_P]
     L.psdm_engine_batch_slots.restype = _I
     L.psdm_engine_check_wait_timeout.argtypes = [_P]
+    CP = C.POINTER(Conditioning)
+    L.psdm_trace_windows.argtypes = [CP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _i32p, _i32p, _i32p]
+    L.psdm_trace_windows.restype = None
+    L.psdm_condition_traces.argtypes = [_P, CP, _I, _f32p, _I, _F, _F, _i32p, _i32p, _i32p, _f32p]
+    L.psdm_condition_traces_device.argtypes = [_P, CP, _I, _P, _I, _F, _F, _i32p, _i32p, _i32p, _P]
     L.psdm_fd_coef.argtypes = [_I, _I, _f32p]
     L.psdm_fd_coef.restype = None
     L.psdm_pml_coeffs.argtypes = [_I, _I, _F, _F, _I, _f32p, _f32p, _P]

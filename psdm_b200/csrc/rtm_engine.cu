@@ -1339,6 +1339,68 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
 
 int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
 
+int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int32_t NumRec,
+                                 const float* d_Field_Data, int32_t nt_data, float dt_data, float dt_prop,
+                                 const int32_t* nt_cut, const int32_t* nt_sf, const int32_t* lens,
+                                 float* d_Data_target) {
+    TRY(check_engine(e));
+    if (!c || !d_Field_Data || !nt_cut || !nt_sf || !lens || !d_Data_target || NumRec < 0)
+        return fail(PSDM_ERR_ARG, "null argument");
+    const int nt_prop2 = lens[0], nt_taper = lens[1], N_taper = lens[2], N_zeros = lens[3];
+    if (nt_data < 1 || nt_prop2 < 0 || nt_taper < nt_prop2 || N_taper < 1 || N_zeros < 0)
+        return fail(PSDM_ERR_ARG, "inconsistent trace lengths");
+    if (dt_data != dt_prop && (dt_data <= 0.f || dt_prop <= 0.f)) return fail(PSDM_ERR_ARG, "time steps must be > 0");
+    if (NumRec == 0) return PSDM_OK;
+    int *d_cut = nullptr, *d_sf = nullptr;
+    float* d_w = nullptr;
+    TRY(e->get("cond_cut", (size_t)NumRec, &d_cut));
+    TRY(e->get("cond_sf", (size_t)NumRec, &d_sf));
+    TRY(e->get("cond_w", (size_t)N_taper, &d_w));
+    std::vector<float> w(N_taper);
+    for (int n = 0; n < N_taper; ++n) w[n] = taper_weight(n, N_taper);
+    CUDA_TRY(cudaMemcpyAsync(d_cut, nt_cut, NumRec * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_sf, nt_sf, NumRec * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_w, w.data(), N_taper * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CondArgs a;
+    a.field = d_Field_Data;
+    a.out = d_Data_target;
+    a.nt_cut = d_cut;
+    a.nt_sf = d_sf;
+    a.w = d_w;
+    a.nrec = NumRec;
+    a.nt_data = nt_data;
+    a.nt_prop2 = nt_prop2;
+    a.nt_taper = nt_taper;
+    a.N_taper = N_taper;
+    a.N_zeros = N_zeros;
+    a.cut_multiple = c->cut_multiple;
+    a.cut_sf = c->cut_sf;
+    a.taper_option = c->taper_option;
+    a.resample = dt_data != dt_prop ? 1 : 0;
+    a.dt_data = dt_data;
+    a.dt_prop = dt_prop;
+    const int rc = launch_condition(a, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "conditioning launch: %s", cudaGetErrorString((cudaError_t)rc));
+    e->launches += 1;
+    return PSDM_OK;
+}
+
+int psdm_condition_traces(psdm_engine* e, const psdm_conditioning* c, int32_t NumRec, const float* Field_Data,
+                          int32_t nt_data, float dt_data, float dt_prop, const int32_t* nt_cut, const int32_t* nt_sf,
+                          const int32_t* lens, float* Data_target) {
+    TRY(check_engine(e));
+    if (!Field_Data || !Data_target || !lens || NumRec < 0) return fail(PSDM_ERR_ARG, "null argument");
+    if (NumRec == 0) return PSDM_OK;
+    const size_t nin = (size_t)NumRec * nt_data, nout = (size_t)NumRec * lens[1];
+    float *d_in = nullptr, *d_out = nullptr;
+    TRY(e->get("cond_in", nin, &d_in));
+    TRY(e->get("cond_out", std::max<size_t>(nout, 1), &d_out));
+    CUDA_TRY(cudaMemcpyAsync(d_in, Field_Data, nin * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    TRY(psdm_condition_traces_device(e, c, NumRec, d_in, nt_data, dt_data, dt_prop, nt_cut, nt_sf, lens, d_out));
+    CUDA_TRY(cudaMemcpyAsync(Data_target, d_out, nout * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    return sync(e);
+}
+
 int psdm_engine_check_wait_timeout(psdm_engine* e) {
     TRY(check_engine(e));
     TRY(sync(e));

@@ -9,6 +9,7 @@
 //   psdm_taper_pad_trace  src/filters.f90:20-48
 //   psdm_optimization_dt  src/optimization.f90:24-32
 //   psdm_normalize_psdm   src/auxiliar_PSDM.f90:1-20
+//   psdm_trace_windows    src/calculate_PSDM_RTM.f90:231-291
 
 #include <algorithm>
 #include <cmath>
@@ -165,6 +166,45 @@ void psdm_dynamic_window(int32_t NumRec, int32_t nxSou, const int32_t* nxRec, fl
     *x_i = xi;
     *x_f = xf;
     *nx_w = xf - xi + 1;
+}
+
+void psdm_trace_windows(const psdm_conditioning* c, int32_t NumRec, int32_t nxSou, int32_t nySou,
+                        const int32_t* nxRec, const int32_t* nyRec, const float* Batmodel, float dmodel_prop,
+                        float dt_prop, int32_t nt_prop, int32_t* nt_cut, int32_t* nt_sf, int32_t* lens) {
+    // Defaults of calculate_PSDM_RTM.f90:123-124 and :64-65.
+    for (int j = 0; j < NumRec; ++j) {
+        nt_cut[j] = nt_prop;
+        nt_sf[j] = 1;
+    }
+    // Half the source-receiver offset and the mean depth below source and
+    // receiver of the sea floor at the midpoint: the legs of the sea-floor
+    // reflection (:233-251 for the multiple, :259-277 for the direct wave).
+    auto leg = [&](int j) {
+        const float offset = fabsf(float(nxSou) * dmodel_prop - float(nxRec[j]) * dmodel_prop);
+        const int mid_x = (int)ceilf(0.5f * float(nxSou + nxRec[j]));
+        const float bat = Batmodel[mid_x - 1];
+        const float D_src = bat - float(nySou) * dmodel_prop;
+        const float D_rec = bat - float(nyRec[j]) * dmodel_prop;
+        const float half = offset * 0.5f, depth = 0.5f * (D_src + D_rec);
+        return sqrtf(half * half + depth * depth);
+    };
+    if (c->cut_multiple > 0)
+        for (int j = 0; j < NumRec; ++j) nt_cut[j] = (int)ceilf((0.9f * ((4.0f * leg(j)) / 1500.f)) / dt_prop);
+    if (c->cut_sf > 0)
+        for (int j = 0; j < NumRec; ++j) nt_sf[j] = (int)ceilf((1.1f * ((2.0f * leg(j)) / 1500.f)) / dt_prop);
+    int nt_prop2 = nt_prop, nt_taper = nt_prop, N_taper = 1, N_zeros = 0;
+    if (c->taper_option != 0 || c->cut_multiple != 0) {  // :286-291
+        N_taper = std::max(1, (int)(c->T_taper / dt_prop));
+        N_zeros = std::max(0, (int)(c->T_zeros / dt_prop));
+        int mx = NumRec > 0 ? nt_cut[0] : nt_prop;
+        for (int j = 1; j < NumRec; ++j) mx = std::max(mx, (int)nt_cut[j]);
+        nt_prop2 = std::min((int)nt_prop, mx);
+        nt_taper = nt_prop2 + N_zeros;
+    }
+    lens[0] = nt_prop2;
+    lens[1] = nt_taper;
+    lens[2] = N_taper;
+    lens[3] = N_zeros;
 }
 
 void psdm_taper_pad_trace(float* trace, int32_t nt_prop, int32_t N_taper, int32_t N_zeros, int32_t nt_new) {

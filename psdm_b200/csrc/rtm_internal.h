@@ -137,6 +137,20 @@ int launch_step(int mode, const StepArgs& a, void* stream);
 // Quantize one snapshot outside a step launch (see StepArgs::q_*).
 int launch_quantize(const float* src, const unsigned int* amax, void* dst, float* iscale, int n, int kind16,
                     void* stream);
+// Trace conditioning (rtm_condition.cu): Data_target (nt_taper per trace)
+// from Field_Data (nt_data per trace); w = taper weights (N_taper).
+struct CondArgs {
+    const float* field;
+    float* out;
+    const int* nt_cut;
+    const int* nt_sf;
+    const float* w;
+    int nrec, nt_data, nt_prop2, nt_taper, N_taper, N_zeros;
+    int cut_multiple, cut_sf, taper_option, resample;
+    float dt_data, dt_prop;
+};
+int launch_condition(const CondArgs& c, void* stream);
+
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
 int launch_wait_timeout_probe(int* err, void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.

@@ -193,6 +193,21 @@ class Engine:
                                               dt, ny, nx, added_space, store_snap, taper_option, N_taper, N_zeros,
                                               max_slots))
 
+    def condition_traces(self, cond, Field_Data, dt_data, dt_prop, nt_cut, nt_sf, lens):
+        """psdm_condition_traces: Data_target (NumRec, nt_taper) from Field_Data (NumRec, nt_data)."""
+        F = _f32(Field_Data)
+        nrec, nt_data = F.shape
+        out = np.zeros((nrec, int(lens[1])), dtype=np.float32)
+        L.check(L.lib().psdm_condition_traces(self._h, C.byref(cond), nrec, F.reshape(-1), nt_data, dt_data, dt_prop,
+                                              _i32(nt_cut), _i32(nt_sf), _i32(lens), out))
+        return out
+
+    def condition_traces_device(self, cond, nrec, d_Field_Data: int, nt_data, dt_data, dt_prop, nt_cut, nt_sf, lens,
+                                d_Data_target: int):
+        """psdm_condition_traces_device (device pointers; asynchronous)."""
+        L.check(L.lib().psdm_condition_traces_device(self._h, C.byref(cond), nrec, d_Field_Data, nt_data, dt_data,
+                                                     dt_prop, _i32(nt_cut), _i32(nt_sf), _i32(lens), d_Data_target))
+
     def check_wait_timeout(self):
         """psdm_engine_check_wait_timeout: raises PsdmError when the failure path works."""
         L.check(L.lib().psdm_engine_check_wait_timeout(self._h))
@@ -257,6 +272,18 @@ def optimization_dt(dmodel_prop: float, vmax: float, tfin: float, store_snap: in
     dt, ntp, nts = C.c_float(), C.c_int32(), C.c_int32()
     L.lib().psdm_optimization_dt(dmodel_prop, vmax, tfin, store_snap, C.byref(dt), C.byref(ntp), C.byref(nts))
     return dt.value, ntp.value, nts.value
+
+
+def trace_windows(cond, nxSou, nySou, nxRec, nyRec, Batmodel, dmodel_prop, dt_prop, nt_prop):
+    """psdm_trace_windows: (nt_cut, nt_sf, lens = [nt_prop2, nt_taper, N_taper, N_zeros])."""
+    nxRec = _i32(nxRec)
+    n = nxRec.size
+    nt_cut = np.zeros(n, np.int32)
+    nt_sf = np.zeros(n, np.int32)
+    lens = np.zeros(4, np.int32)
+    L.lib().psdm_trace_windows(C.byref(cond), n, int(nxSou), int(nySou), nxRec, _i32(nyRec), _f32(Batmodel),
+                               dmodel_prop, dt_prop, nt_prop, nt_cut, nt_sf, lens)
+    return nt_cut, nt_sf, lens
 
 
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
