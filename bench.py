@@ -236,6 +236,60 @@ FORMS = [
 ]
 
 
+def time_conditioning(engine, torch, dev, stream, survey, nshot_traces=480):
+    """Device time of the trace conditioning of one shot (480 traces of 2 s at
+    2 ms resampled to the 0.5 ms propagation step, sea-floor and multiple cuts,
+    taper), against the CPU restatement on one core."""
+    from psdm_b200 import rtm
+    from psdm_b200._lib import Conditioning
+    from oracle import oracle as O
+    vel = synth_model_cached()
+    bat = np.zeros(NX, np.float32)
+    for i in range(NX):
+        j = np.flatnonzero(vel[i] > 1500.0)
+        bat[i] = np.float32(j[0] - 1) * np.float32(DD) if j.size else 0.0
+    cond = Conditioning(1, 1, 1, 0.05, 0.2)
+    s = 0
+    cut, sf, lens = rtm.trace_windows(cond, survey.nxSou[s], survey.nySou[s], survey.nxRec[s], survey.nyRec[s], bat,
+                                      DD, DT, NT)
+    dt_data = 4 * DT
+    nt_data = NT // 4 + 4
+    F = np.cumsum(np.random.default_rng(3).standard_normal((len(cut), nt_data)), axis=1).astype(np.float32)
+    d_in = torch.from_numpy(F).to(dev)
+    d_out = torch.zeros((len(cut), int(lens[1])), dtype=torch.float32, device=dev)
+    run = lambda: engine.condition_traces_device(cond, len(cut), d_in.data_ptr(), nt_data, dt_data, DT, cut, sf, lens,
+                                                 d_out.data_ptr())
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    gpu_ms = e0.elapsed_time(e1) / reps
+    t0 = time.perf_counter()
+    O.condition_traces(cut_multiple=1, cut_sf=1, taper_option=1, Field_Data=F, dt_data=dt_data, dt_prop=DT,
+                       nt_prop2=int(lens[0]), nt_taper=int(lens[1]), N_taper=int(lens[2]), N_zeros=int(lens[3]),
+                       nt_cut=cut, nt_sf=sf)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    return {"gpu_ms_per_shot": gpu_ms, "cpu_ms_per_shot": cpu_ms, "cpu_cores": 1, "traces": len(cut),
+            "samples_in": nt_data, "samples_out": int(lens[1]), "api": "psdm_condition_traces_device"}
+
+
+_VEL = None
+
+
+def synth_model_cached():
+    global _VEL
+    if _VEL is None:
+        from psdm_b200 import synth
+        _VEL = synth.config2_model(seed=2)
+    return _VEL
+
+
 def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
     """Shots/s of each named form on the workload's shots (inputs in HBM)."""
     from psdm_b200 import rtm
@@ -319,7 +373,7 @@ def run_gpu(args):
     prm = rtm.Params(dPML=DPML, fs=1, strategy=1)
 
     survey = synth.config2_survey(200)
-    vel_true = synth.config2_model(seed=2)
+    vel_true = synth_model_cached()
     vel_mig = synth.smooth_model(vel_true, 100.0, DD)
     n_total = args.warmup + args.steps
     # round-robin shots (0-based lines, wrapping over the survey)
@@ -407,6 +461,9 @@ def run_gpu(args):
     names = [f[0] for f in FORMS] if args.forms == "all" else [n for n in args.forms.split(",") if n and n != "none"]
     if world == 1 and names:
         forms = time_forms(engine, torch, dev, stream, d_src, items_u, names, value)
+    conditioning = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        conditioning = time_conditioning(engine, torch, dev, stream, survey)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -435,6 +492,7 @@ def run_gpu(args):
                 "clocks": clk.summary(),
                 "e2e": e2e,
                 "forms": forms,
+                "conditioning": conditioning,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if world > 1:

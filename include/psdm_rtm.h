@@ -308,6 +308,30 @@ int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int
                                  float dt_prop, const int32_t* nt_cut, const int32_t* nt_sf,
                                  const int32_t* lens, float* d_Data_target);
 
+/* ---- SU trace files without the SU tools ---------------------------------- */
+
+/*
+ * Write model(nj, ni) as ni SU traces of nj samples with the headers the
+ * reference's write_psdm / write_vel pipelines set (src/auxiliar.f90:275-353,
+ * a2b | suaddhead | sushw | suchw): tracl = tracr = 1..ni, ns = nj, d1 = dj,
+ * f1 = 0, d2 = di, f2 = 0, cdp = -di + di*tracl, trid.  big_endian != 0
+ * writes big-endian words.
+ */
+int psdm_su_write_image(const char* path, int32_t ni, int32_t nj, float di, float dj, int32_t trid,
+                        const float* model, int32_t big_endian);
+/*
+ * Read NumRec fixed-length SU traces (240-byte header + ns_max samples) as
+ * get_shot_data does (src/get_mcs_data.f90:150-214): raw (nt, NumRec) gets
+ * samples 1..nt of each trace; delayed (nt, NumRec, or NULL) gets them shifted
+ * by delay_samples (later for > 0), zero where nothing lands.
+ */
+int psdm_su_read_shot(const char* path, int32_t NumRec, int32_t ns_max, int32_t nt, int32_t big_endian,
+                      int32_t delay_samples, float* raw, float* delayed);
+/* The int32 header word at 1-based byte position byte_pos of each of NumRec
+ * fixed-length traces (shot number, offset: get_mcs_data.f90:449-470). */
+int psdm_su_read_header_i32(const char* path, int32_t NumRec, int32_t ns_max, int32_t byte_pos,
+                            int32_t big_endian, int32_t* out);
+
 /* normalize_psdm (src/auxiliar_PSDM.f90:1-20): PSDM = sum/fold where fold > 0. */
 void psdm_normalize_psdm(int32_t nx, int32_t ny, const float* PSDM_sum, const float* Cov_sum,
                          float* PSDM);

@@ -286,6 +286,29 @@ def trace_windows(cond, nxSou, nySou, nxRec, nyRec, Batmodel, dmodel_prop, dt_pr
     return nt_cut, nt_sf, lens
 
 
+def su_write_image(path: str, model, di: float, dj: float, trid: int = 200, big_endian: bool = False):
+    """psdm_su_write_image: model (ni, nj) in C order (the reference's (nj, ni)) as ni SU traces."""
+    m = _f32(model)
+    ni, nj = m.shape
+    L.check(L.lib().psdm_su_write_image(str(path).encode(), ni, nj, di, dj, trid, m.reshape(-1), int(big_endian)))
+
+
+def su_read_shot(path: str, nrec: int, ns_max: int, nt: int, big_endian: bool = False, delay_samples: int = 0):
+    """psdm_su_read_shot: (raw, delayed), each (nrec, nt)."""
+    raw = np.zeros((nrec, nt), np.float32)
+    delayed = np.zeros((nrec, nt), np.float32)
+    L.check(L.lib().psdm_su_read_shot(str(path).encode(), nrec, ns_max, nt, int(big_endian), delay_samples, raw,
+                                      delayed.ctypes.data))
+    return raw, delayed
+
+
+def su_read_header_i32(path: str, nrec: int, ns_max: int, byte_pos: int, big_endian: bool = False):
+    """psdm_su_read_header_i32: the int32 word at 1-based byte byte_pos of each trace."""
+    out = np.zeros(nrec, np.int32)
+    L.check(L.lib().psdm_su_read_header_i32(str(path).encode(), nrec, ns_max, byte_pos, int(big_endian), out))
+    return out
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a, b = _f32(psdm_sum), _f32(cov_sum)
     out = np.zeros_like(a)
