@@ -76,8 +76,6 @@ constexpr int ZTX = NWARP * ZXS;
 constexpr int ZWX = ZTX + 6;
 constexpr int RTX = 64;
 constexpr int NT = 32 * NWARP;  // threads per block
-// C-PML strip tiles also stage their phi tile, after the p tile.
-constexpr int PHI_OFF = WX * HZ;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -639,10 +637,6 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     const int sz0 = z0 - 4;
     const int sx0 = min(x0, a.nxt - 4) - 3;
     load_tile(a, ps, sz0, sx0, HQ, PWX, tid);
-    // phi columns: x0-6 .. x0+21 covers ci-3 .. ci+3 for every column of the
-    // tile, ci being clamped into the strip.
-    const int sxp = x0 - 6;
-    load_tile_from(a.phix_in, a, ps + PHI_OFF, sz0, sxp, HQ, PTX + 12, tid);
     __syncthreads();
     const int zd = z0 + 4 * lane;
     if (zd >= zend) return;
@@ -650,7 +644,6 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     const int z = zd - a.zoff;
     const bool fsq = a.fs && z == dn;
     const float4* __restrict__ ps4 = reinterpret_cast<const float4*>(ps);
-    const float4* __restrict__ ph4 = reinterpret_cast<const float4*>(ps + PHI_OFF);
     const int qr = (zd - sz0) >> 2;
     const float* c1 = a.cf1;
     const float* c2 = a.cf2;
@@ -673,9 +666,9 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
         float4 F[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k)
-            if (k != 3) F[k] = ph4[(ci + k - 3 - sxp) * HQ + qr];
+            if (k != 3) F[k] = __ldg(reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd));
         F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 phc = ph4[(x - sxp) * HQ + qr];
+        const float4 phc = __ldg(reinterpret_cast<const float4*>(a.phix_in + g));
         const float4 chc = *reinterpret_cast<const float4*>(a.chix + g);
         const float4 pmv = *reinterpret_cast<const float4*>(a.pm + g);
         const float4 c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
@@ -724,9 +717,6 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     const int sz0 = (min(z0, nr - 4) - 3) & ~3;
     const int sx0 = x0 - 3;  // interior columns: no clamping along x
     load_tile(a, ps, sz0, sx0, PHQ, ZWX, tid);
-    // phi rows: 4 more above the p tile, so that cj-3 stays inside when a
-    // tile starts within 3 rows of a strip's end.
-    load_tile_from(a.phiz_in, a, ps + PHI_OFF, sz0 - 4, sx0, PHQ + 1, ZWX, tid);
     __syncthreads();
     const int zd = z0 + lane;
     if (zd >= zend) return;
@@ -764,12 +754,12 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
         const float d1 = D1(AZ, c1);
 #undef AX
         const int g = x * a.ldz + zd;
-        const float* phs = ps + PHI_OFF + xl * (PHZ + 4) + 4 - sz0;
-#define PZ(k) phs[cj + (k)]
+        const float* phs = a.phiz_in + x * a.ldz;
+#define PZ(k) __ldg(phs + cj + (k))
         const float dph = D1(PZ, c1);
 #undef PZ
 #undef AZ
-        const float phn = __fadd_rn(__fmul_rn(A, phs[zd]), __fmul_rn(B, d1));
+        const float phn = __fadd_rn(__fmul_rn(A, __ldg(phs + zd)), __fmul_rn(B, d1));
         const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
         a.phiz_out[g] = phn;
         a.chiz[g] = chn;
@@ -805,7 +795,7 @@ __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r
 
 template <int MODE>
 constexpr int smem_floats() {
-    return PHI_OFF + HZ * (PTX + 12);  // p tile; phi tile of the C-PML strip tiles
+    return WX * HZ;  // the p tile of an interior tile (boundary tiles use less)
 }
 
 template <int MODE>
