@@ -233,6 +233,7 @@ FORMS = [
     ("batch_fp16_ks4", 1, 4, 8),
     ("batch_bf16_ks4", 2, 4, 8),
     ("batch_fp32", 0, 1, 2),
+    ("fp32_checkpoint_k100", 0, 1, -100),  # slots < 0: one shot at a time, checkpoint interval -slots
 ]
 
 
@@ -299,7 +300,10 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         if name not in names:
             continue
         prm = rtm.Params(dPML=DPML, fs=1, strategy=1, precision=precision)
+        ckpt = -slots if slots < 0 else 0
+        slots = max(slots, 0)
         n = 2 * slots if slots else 4
+        engine.set_checkpointing(ckpt)
         sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
 
         def run(k):
@@ -322,10 +326,13 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         run(n)
         e1.record(stream)
         torch.cuda.synchronize(dev)
+        engine.set_checkpointing(0)
         v = n / (e0.elapsed_time(e1) / 1e3)
         out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
                      "slots": engine.batch_slots() if slots else 1, "precision": ["f32", "fp16", "bf16"][precision],
                      "store_snap": ks}
+        if ckpt:
+            out[name]["checkpoint_interval"] = ckpt
     return out
 
 

@@ -186,6 +186,17 @@ int psdm_rtm_batch_device(
     psdm_engine* e, const psdm_params* prm, int32_t nshots, const psdm_shot* shots,
     const float* d_Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
     int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots);
+/*
+ * Checkpointing for FP32 shots (psdm_rtm_shot, psdm_rtm_shot_device):
+ * interval K > 0 keeps the propagation state every K forward steps and
+ * recomputes each K-step segment of the forward pass during the backward
+ * pass, in place of holding all nt_prop2 snapshots (the role of the
+ * reference's disk strategy, solver_ac_forward_disk.f90:469-517).  Same image
+ * bit for bit; the forward pass runs twice.  0 (default) = off.  Not used by
+ * the batched or mixed-precision forms.
+ */
+int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval);
+
 /* Shots in flight at a time in the last batched call. */
 int32_t psdm_engine_batch_slots(const psdm_engine* e);
 

@@ -24,7 +24,7 @@ EXPORTS = [
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
     "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
     "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
-    "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32",
+    "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing",
 ]
 
 
@@ -99,6 +99,7 @@ def lib():
     L.psdm_engine_batch_slots.argtypes = [_P]
     L.psdm_engine_batch_slots.restype = _I
     L.psdm_engine_check_wait_timeout.argtypes = [_P]
+    L.psdm_engine_set_checkpointing.argtypes = [_P, _I]
     L.psdm_su_write_image.argtypes = [C.c_char_p, _I, _I, _F, _F, _I, _f32p, _I]
     L.psdm_su_read_shot.argtypes = [C.c_char_p, _I, _I, _I, _I, _I, _f32p, _P]
     L.psdm_su_read_header_i32.argtypes = [C.c_char_p, _I, _I, _I, _I, _i32p]

@@ -81,6 +81,7 @@ struct psdm_engine {
     } graphs[3];
     bool use_graphs = true;
     int batch_slots = 0;  // slots used by the last batched call
+    int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
@@ -498,7 +499,8 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
 //   taper weight of slot `snap` (size >= nt_snap; null for all ones).
 int build_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
                    int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
-                   const float* h_w, float* d_image, const std::string& tag, std::vector<StepArgs>* steps_out) {
+                   const float* h_w, float* d_image, const std::string& tag, std::vector<StepArgs>* steps_out,
+                   std::vector<int>* slot_of_step = nullptr) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, nrec, zr, xr, &inj));
@@ -522,14 +524,17 @@ int build_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap,
         a.inj_t = reverse ? nt - k + 1 : k - 2;  // Sadj(k-1)
         a.field = nullptr;
         a.field_w = 1.f;
+        int used = 0;
         if ((k - 1) % store_snap == 0) {
             snap = snap - 1;
             if (d_fields && snap >= slot_lo && snap <= slot_hi && snap >= 1) {
                 a.field = const_cast<float*>(d_fields) + (size_t)(snap - slot_lo) * fstride;
                 a.field_w = h_w ? h_w[snap - 1] : 1.f;
                 if (a.field_w == 0.f) a.field = nullptr;  // zero-padded slot: no contribution
+                if (a.field) used = snap;
             }
         }
+        if (slot_of_step) slot_of_step->push_back(used);
         steps.push_back(a);
     }
     return PSDM_OK;
@@ -717,6 +722,121 @@ std::vector<float> taper_weights(int nt_prop2, int nt_taper, int taper_option, i
     return wts;
 }
 
+// ---- checkpointed FP32 shot ------------------------------------------------------
+//
+// In place of keeping every snapshot of the forward pass (the RAM strategy)
+// or writing them to files (the disk strategy, solver_ac_forward_disk.f90:
+// 469-517), the forward pass keeps the whole propagation state every K steps
+// (p at both levels, the C-PML variables, the free-surface histories), and
+// the backward pass recomputes each K-step segment of the forward pass from
+// its checkpoint into a K-slot buffer just before it needs the segment's
+// snapshots, visiting the segments from last to first.  The kernels and
+// their arguments are those of the plain shot, so the image is the same bit
+// for bit; the forward pass runs twice.  Memory: (segments - 1) states plus
+// K snapshots instead of nt_prop2 snapshots.
+
+struct StateView {
+    float* a[10];
+    size_t n[10];
+};
+
+StateView state_of(Shot& s) {
+    const size_t n = s.g.cells(), m = (size_t)s.g.nxt;
+    return StateView{{s.p[0], s.p[1], s.phx[0], s.phx[1], s.chx, s.phz[0], s.phz[1], s.chz, s.side[0], s.side[1]},
+                     {n, n, n, n, n, n, n, n, m, m}};
+}
+
+size_t state_floats(const Shot& s) { return 8 * s.g.cells() + 2 * (size_t)s.g.nxt; }
+
+int copy_state(psdm_engine* e, Shot& s, float* ck, bool save) {
+    const StateView v = state_of(s);
+    size_t off = 0;
+    for (int i = 0; i < 10; ++i) {
+        float* dst = save ? ck + off : v.a[i];
+        const float* src = save ? v.a[i] : ck + off;
+        CUDA_TRY(cudaMemcpyAsync(dst, src, v.n[i] * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+        off += v.n[i];
+    }
+    if (!save) CUDA_TRY(cudaMemsetAsync(s.counters, 0, 2 * sizeof(int), e->stream));
+    return PSDM_OK;
+}
+
+int launch_direct(psdm_engine* e, int mode, const StepArgs& a) {
+    const int rc = launch_step(mode, a, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)rc));
+    e->launches += 1;
+    return PSDM_OK;
+}
+
+int rtm_shot_checkpointed(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
+                          const int* nyRec, const float* d_S, const float* d_tgt, float dd, float dt, int ny, int nx,
+                          int nx_w, const float* d_vp, float added_space, int store_snap, int nt_prop2, int nt_taper,
+                          const float* wts, float* d_img, int K) {
+    Shot f, b;  // forward (recomputed) and backward states
+    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &f, "_ckf"));
+    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &b));
+    WinGeom w;
+    TRY(window_geometry(f.g, NumRec, nxSou, nySou, nxRec, nyRec, dd, nx, added_space, &w));
+    if (w.nx_w_calc != nx_w)
+        return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
+    const size_t fstride = f.g.field_cells();
+    const int nsteps = nt_prop2 - 1, nseg = (nsteps + K - 1) / K;
+    const int nsnap = (nt_prop2 - 1) / store_snap;
+    float *segbuf = nullptr, *ckpts = nullptr, *d_imgp = nullptr;
+    TRY(e->get("ck_segment", fstride * (size_t)K, &segbuf));
+    const size_t sf = state_floats(f);
+    if (nseg > 1) TRY(e->get("ck_states", sf * (size_t)(nseg - 1), &ckpts));
+    TRY(e->get("image_pitched", fstride, &d_imgp));
+    TRY(e->record(0));
+    // Forward steps: without snapshots (first pass), and with the snapshot
+    // of step k in segment slot (k-2) % K (recomputation).
+    std::vector<StepArgs> fwd;
+    TRY(build_forward(e, f, nt_prop2, store_snap, d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, "_ckf", &fwd));
+    for (int i = 0; i < nsteps; ++i) {
+        if (i > 0 && i % K == 0) TRY(copy_state(e, f, ckpts + sf * (size_t)(i / K - 1), true));
+        TRY(launch_direct(e, 0, fwd[i]));
+    }
+    e->fwd_steps += nsteps;
+    TRY(e->record(1));
+    // Backward steps, with each imaging step's slot remapped into the segment buffer.
+    std::vector<StepArgs> bwd;
+    std::vector<int> slot;
+    CUDA_TRY(cudaMemsetAsync(d_imgp, 0, fstride * sizeof(float), e->stream));
+    TRY(build_backward(e, b, nt_taper, store_snap, nt_taper, d_tgt, 1, NumRec, w.zr.data(), w.xr.data(), segbuf, 1,
+                       nsnap, wts, d_imgp, "", &bwd, &slot));
+    int cur = -1;
+    for (size_t i = 0; i < bwd.size(); ++i) {
+        const int m = slot[i];
+        if (m > 0) {
+            const int kf = store_snap * m + 1;  // forward step that took slot m
+            const int j = (kf - 2) / K;
+            if (j != cur) {  // recompute segment j from its checkpoint
+                if (j == 0)
+                    TRY(reset_state(e, &f));
+                else
+                    TRY(copy_state(e, f, ckpts + sf * (size_t)(j - 1), false));
+                const int i1 = std::min((j + 1) * K, nsteps);
+                for (int t = j * K; t < i1; ++t) {
+                    StepArgs a = fwd[t];
+                    const int k = t + 2;
+                    if ((k - 1) % store_snap == 0 && (k - 1) / store_snap <= nsnap)
+                        a.field = segbuf + (size_t)(t - j * K) * fstride;
+                    TRY(launch_direct(e, 0, a));
+                }
+                e->fwd_steps += i1 - j * K;
+                cur = j;
+            }
+            bwd[i].field = segbuf + (size_t)(kf - 2 - j * K) * fstride;
+        }
+        TRY(launch_direct(e, 1, bwd[i]));
+    }
+    e->bwd_steps += (int64_t)bwd.size();
+    TRY(e->record(2));
+    CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)b.g.ldf * sizeof(float),
+                               (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
+    return PSDM_OK;
+}
+
 // One shot of RTM with every array in device memory
 // (calculate_PSDM_RTM.f90:395-466).  Asynchronous on e->stream.
 int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
@@ -769,6 +889,12 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
         CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
                                    (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
         return PSDM_OK;
+    }
+    if (e->ckpt_interval > 0) {
+        const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, taper_option, N_taper, N_zeros);
+        return rtm_shot_checkpointed(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_S, d_tgt, dd, dt, ny, nx, nx_w,
+                                     d_vp, added_space, store_snap, nt_prop2, nt_taper, wts.data(), d_img,
+                                     e->ckpt_interval);
     }
     if (nsnap > 0) TRY(e->get("fields", fstride * nsnap, &d_F));
     TRY(e->record(0));
@@ -1338,6 +1464,14 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
 }
 
 int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
+
+int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval) {
+    TRY(check_engine(e));
+    if (interval < 0) return fail(PSDM_ERR_ARG, "checkpoint interval must be >= 0");
+    TRY(sync(e));
+    e->ckpt_interval = interval;
+    return PSDM_OK;
+}
 
 int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int32_t NumRec,
                                  const float* d_Field_Data, int32_t nt_data, float dt_data, float dt_prop,

@@ -208,6 +208,10 @@ class Engine:
         L.check(L.lib().psdm_condition_traces_device(self._h, C.byref(cond), nrec, d_Field_Data, nt_data, dt_data,
                                                      dt_prop, _i32(nt_cut), _i32(nt_sf), _i32(lens), d_Data_target))
 
+    def set_checkpointing(self, interval: int):
+        """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
+        L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))
+
     def check_wait_timeout(self):
         """psdm_engine_check_wait_timeout: raises PsdmError when the failure path works."""
         L.check(L.lib().psdm_engine_check_wait_timeout(self._h))
