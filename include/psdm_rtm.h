@@ -43,7 +43,7 @@ enum {
 /*
  * Values the reference solvers read from module mod_parfile
  * (src/solver_ac_forward_ram.f90:8 `USE mod_parfile, ONLY: dPML, fs`) and
- * the driver's strategy switch (src/calculate_PSDM_RTM.f90:395,411,435).
+ * the strategy switch of calculate_PSDM_RTM (src/calculate_PSDM_RTM.f90:395,411,435).
  */
 typedef struct psdm_params {
     int32_t dPML;       /* C-PML thickness in cells (parfile `dPML`, default 20) */

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (liboracle_rtm.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, and only as the checker.  The CUDA engine in
+CPU-baseline leg of bench.py, and only to check the engine against.  The CUDA engine in
 psdm_b200/ never imports this module.
 
 The oracle restates the reference's Fortran RTM solvers step by step (see the

@@ -1,6 +1,6 @@
 // CPU oracle for the PSDM reverse-time-migration (RTM) propagators.
 //
-// TEST INFRASTRUCTURE ONLY.  This file is the checker, never the product:
+// TEST INFRASTRUCTURE ONLY.  The engine is checked against it; it is never the product:
 // only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
 // it.  The CUDA engine in psdm_b200/ never links or calls it.
 //

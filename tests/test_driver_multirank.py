@@ -1,4 +1,4 @@
-"""Shot loop of the driver on two CPU ranks (gloo), against the same loop
+"""Shot loop of psdm_b200.driver on two CPU ranks (gloo), against the same loop
 evaluated serially.
 
 The shot loop deals shots round-robin (calculate_PSDM_RTM.f90:164-166),
