@@ -319,6 +319,21 @@ int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int
                                  float dt_prop, const int32_t* nt_cut, const int32_t* nt_sf,
                                  const int32_t* lens, float* d_Data_target);
 
+/*
+ * The frequency filter of the data preparation (freq_filter, src/auxiliar.f90:
+ * 498-531, with filters_function1D and butterworth, src/filters.f90:50-232) on
+ * the GPU, in place on traces (nt, Num): order-6 Butterworth low-pass
+ * (typef 1, cut-off f2), high-pass (2, from 40 Hz as the reference fixes it)
+ * or band-pass (3, f1..f2), applied through a 24-times zero-padded FFT;
+ * all-zero traces are left as they are.  The transforms are cuFFT's, so the
+ * result matches the reference's FFTPACK arithmetic to FP32 rounding.
+ */
+int psdm_freq_filter(psdm_engine* e, float* traces, int32_t nt, float dt, int32_t Num, int32_t typef,
+                     float f1, float f2);
+/* Same on a device array; asynchronous on the engine's stream. */
+int psdm_freq_filter_device(psdm_engine* e, float* d_traces, int32_t nt, float dt, int32_t Num,
+                            int32_t typef, float f1, float f2);
+
 /* ---- SU trace files without the SU tools ---------------------------------- */
 
 /*

@@ -242,6 +242,64 @@ def condition_traces(*, cut_multiple, cut_sf, taper_option, Field_Data, dt_data,
     return out
 
 
+def butterworth_response(ts: int, fe: float, typef: int, f1: float, fc: float) -> np.ndarray:
+    """The order-6 Butterworth response H[ts] of filters_function1D
+    (filters.f90:50-76) and butterworth (filters.f90:129-232, even order):
+    low-pass at fc (typef 1), high-pass from the fixed 40 Hz (2), band-pass
+    f1..fc (3).  Evaluated like the reference, in single precision with the
+    frequency accumulated by fe/ts per bin, then mirrored Hermitian."""
+    f32, c64 = np.float32, np.complex64
+    n, pi, fs = 6, f32(3.14159265), f32(40.0)
+    f1, fc, fe = f32(f1), f32(fc), f32(fe)
+    f0 = np.sqrt(f1 * fc)
+    Q = f0 / (fc - f1)
+    half = ts // 2 + 1
+    freqs = np.zeros(half, f32)
+    f = f32(0.0)
+    step = fe / f32(ts)
+    for j in range(half):  # f = f + fe/ts, accumulated in single precision
+        freqs[j] = f
+        f = f32(f + step)
+    iw = (1j * freqs).astype(c64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if typef == 1:
+            s = iw / fc
+        elif typef == 2:
+            s = fs / iw
+        else:
+            s = Q * (iw / f0 + f0 / iw)
+        Bn = np.ones(half, c64)
+        for k in range(1, n // 2 + 1):
+            c = np.cos(f32(2 * k + n - 1) * pi / f32(2 * n)).astype(f32)
+            Bn = (Bn * (s * s - f32(2.0) * s * c + f32(1.0))).astype(c64)
+        H = np.zeros(ts, c64)
+        H[:half] = (1.0 / Bn).astype(c64)
+    H[0] = 1.0 if typef == 1 else 0.0
+    H[half:] = np.conj(H[1:ts - half + 1][::-1])
+    return H
+
+
+def freq_filter(Data_trace, dt: float, typef: int, f1: float, f2: float) -> np.ndarray:
+    """freq_filter (auxiliar.f90:498-531) on traces (Num, nt), in float64:
+    each trace that is not all zero goes to the end of a zero buffer of
+    24*nt samples, is transformed forward with the 1/n scaling of FFTPACK's
+    cfft1f, multiplied by the response, transformed back unscaled (cfft1b),
+    and the real part of the last nt samples replaces it
+    (filters.f90:78-108)."""
+    D = np.array(Data_trace, dtype=np.float64, copy=True)
+    num, nt = D.shape
+    ts = 24 * nt
+    H = butterworth_response(ts, 1.0 / np.float32(dt), typef, f1, f2).astype(np.complex128)
+    for i in range(num):
+        if not np.any(D[i] != 0.0):
+            continue
+        x = np.zeros(ts, np.float64)
+        x[ts - nt:] = D[i]
+        y = np.fft.ifft(np.fft.fft(x) / ts * H) * ts
+        D[i] = y.real[ts - nt:]
+    return D
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a = _f32(psdm_sum)
     b = _f32(cov_sum)

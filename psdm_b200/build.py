@@ -18,7 +18,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libpsdm_rtm.so")
 INCLUDE = os.path.join(os.path.dirname(PKG), "include")
 
-SOURCES = ["rtm_step.cu", "rtm_engine.cu", "rtm_host.cpp", "rtm_noalloc.cu", "rtm_condition.cu", "su_io.cpp"]
+SOURCES = ["rtm_step.cu", "rtm_engine.cu", "rtm_host.cpp", "rtm_noalloc.cu", "rtm_condition.cu", "su_io.cpp", "rtm_filter.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {s}")
         objs.append(o)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart", "-lcufft"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <complex>
 #include <map>
 #include <string>
 #include <vector>
@@ -82,6 +83,7 @@ struct psdm_engine {
     bool use_graphs = true;
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
+    std::map<std::pair<int, int>, int> fft_plans;  // (length, batch) -> cuFFT plan handle
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
@@ -130,6 +132,8 @@ struct psdm_engine {
     }
     int trim() {
         drop_graphs();
+        for (auto& kv : fft_plans) destroy_fft_plan(&kv.second);
+        fft_plans.clear();
         for (auto& kv : bufs)
             if (kv.second.ptr) CUDA_TRY(cudaFree(kv.second.ptr));
         bufs.clear();
@@ -1532,6 +1536,48 @@ int psdm_condition_traces(psdm_engine* e, const psdm_conditioning* c, int32_t Nu
     CUDA_TRY(cudaMemcpyAsync(d_in, Field_Data, nin * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     TRY(psdm_condition_traces_device(e, c, NumRec, d_in, nt_data, dt_data, dt_prop, nt_cut, nt_sf, lens, d_out));
     CUDA_TRY(cudaMemcpyAsync(Data_target, d_out, nout * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    return sync(e);
+}
+
+int psdm_freq_filter_device(psdm_engine* e, float* d_traces, int32_t nt, float dt, int32_t Num, int32_t typef,
+                            float f1, float f2) {
+    TRY(check_engine(e));
+    if (!d_traces || nt < 1 || Num < 0 || !(dt > 0.f)) return fail(PSDM_ERR_ARG, "null argument or empty trace");
+    if (typef < 1 || typef > 3) return fail(PSDM_ERR_ARG, "typef must be 1 (low-pass), 2 (high-pass) or 3 (band-pass)");
+    if (Num == 0) return PSDM_OK;
+    const int ts = 24 * nt;  // zero_pad = 24 (auxiliar.f90:511-512)
+    std::vector<std::complex<float>> H(ts);
+    butterworth_response(ts, 1.f / dt, typef, f1, f2, H.data());
+    float *d_H = nullptr, *d_x = nullptr;
+    int* d_keep = nullptr;
+    TRY(e->get("filt_H", (size_t)ts * 2, &d_H));
+    TRY(e->get("filt_x", (size_t)ts * Num * 2, &d_x));
+    TRY(e->get("filt_keep", (size_t)Num, &d_keep));
+    CUDA_TRY(cudaMemcpyAsync(d_H, H.data(), (size_t)ts * sizeof(std::complex<float>), cudaMemcpyHostToDevice,
+                             e->stream));
+    auto key = std::make_pair(ts, (int)Num);
+    auto it = e->fft_plans.find(key);
+    if (it == e->fft_plans.end()) {
+        int plan = 0;
+        if (make_fft_plan(ts, Num, &plan)) return fail(PSDM_ERR_CUDA, "cuFFT plan of length %d x %d failed", ts, Num);
+        it = e->fft_plans.emplace(key, plan).first;
+    }
+    const int rc = filter_traces(d_traces, nt, Num, d_H, d_x, d_keep, ts, &it->second, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "frequency filter failed (step %d)", rc);
+    e->launches += 5;
+    return PSDM_OK;
+}
+
+int psdm_freq_filter(psdm_engine* e, float* traces, int32_t nt, float dt, int32_t Num, int32_t typef, float f1,
+                     float f2) {
+    TRY(check_engine(e));
+    if (!traces || nt < 1 || Num < 0) return fail(PSDM_ERR_ARG, "null argument or empty trace");
+    if (Num == 0) return PSDM_OK;
+    float* d = nullptr;
+    TRY(e->get("filt_traces", (size_t)nt * Num, &d));
+    CUDA_TRY(cudaMemcpyAsync(d, traces, (size_t)nt * Num * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    TRY(psdm_freq_filter_device(e, d, nt, dt, Num, typef, f1, f2));
+    CUDA_TRY(cudaMemcpyAsync(traces, d, (size_t)nt * Num * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
     return sync(e);
 }
 

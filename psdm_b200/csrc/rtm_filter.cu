@@ -1,0 +1,120 @@
+// Frequency filter of recorded traces on the device: the reference's
+// freq_filter (src/auxiliar.f90:498-531) with filters_function1D and its
+// order-6 Butterworth response (src/filters.f90:50-232).  Each trace is
+// placed at the end of a zero buffer 24 times its length, transformed,
+// multiplied by the response (and by 1/n, the forward scaling of the
+// reference's FFT), transformed back, and the real part of the last nt
+// samples is kept.  The transforms are cuFFT's (a library FFT, like the
+// reference's vendored FFTPACK); the results agree with the reference's
+// arithmetic to FP32 rounding, not bit for bit.
+
+#include <cuda_runtime.h>
+#include <cuComplex.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include "rtm_internal.h"
+
+namespace psdm {
+
+// Butterworth response H[ts] (butterworth, filters.f90:129-232) for the
+// filter filters_function1D sets up: order n = 6 (even), high-pass start
+// fs = 40 Hz, band edges f1 and fc, f0 = sqrt(f1 fc), Q = f0 / (fc - f1),
+// frequency step fe/ts accumulated in single precision as the reference does.
+void butterworth_response(int ts, float fe, int typef, float f1, float fc, std::complex<float>* H) {
+    using cf = std::complex<float>;
+    const int n = 6;
+    const float pi = 3.14159265f, fs = 40.f;
+    const float f2 = fc;
+    const float f0 = std::sqrt(f1 * f2);
+    const float Q = f0 / (f2 - f1);
+    const cf I(0.f, 1.f);
+    std::vector<cf> Bn(ts, cf(1.f, 0.f));
+    float f = 0.f;
+    for (int j = 0; j < ts / 2 + 1; ++j) {
+        for (int k = 1; k <= n / 2; ++k) {
+            const float c = std::cos((float(2 * k + n - 1) * pi) / float(2 * n));
+            cf s;
+            if (typef == 1)
+                s = (I * f) / fc;
+            else if (typef == 2)
+                s = fs / (I * f);
+            else
+                s = Q * ((I * f) / f0 + f0 / (I * f));
+            Bn[j] = Bn[j] * (s * s - 2.f * s * c + 1.f);
+        }
+        f = f + fe / float(ts);
+    }
+    for (int j = 0; j < ts / 2 + 1; ++j) H[j] = cf(1.f, 0.f) / Bn[j];
+    H[0] = typef == 1 ? cf(1.f, 0.f) : cf(0.f, 0.f);
+    for (int j = 2; j <= ts / 2; ++j) H[ts / 2 + j - 1] = std::conj(H[ts / 2 + 1 - (j - 1) - 1]);
+}
+
+namespace {
+
+__global__ void pad_traces(const float* tr, int nt, int ts, int num, cufftComplex* x) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)ts * num) return;
+    const int t = (int)(i % ts), r = (int)(i / ts);
+    const int off = ts - nt;
+    x[i] = make_cuComplex(t >= off ? tr[(size_t)r * nt + (t - off)] : 0.f, 0.f);
+}
+
+__global__ void apply_response(cufftComplex* x, const cufftComplex* H, int ts, int num, float scale) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)ts * num) return;
+    const cufftComplex h = H[i % ts], v = x[i];
+    const float re = v.x * scale, im = v.y * scale;  // forward transform scaled by 1/ts
+    x[i] = make_cuComplex(re * h.x - im * h.y, re * h.y + im * h.x);
+}
+
+__global__ void unpad_traces(const cufftComplex* x, int nt, int ts, int num, const int* keep, float* tr) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)nt * num) return;
+    const int t = (int)(i % nt), r = (int)(i / nt);
+    if (!keep[r]) return;  // an all-zero trace is left as it is (is_not_cero)
+    tr[i] = x[(size_t)r * ts + (ts - nt) + t].x;
+}
+
+__global__ void nonzero_traces(const float* tr, int nt, int num, int* keep) {
+    const int r = blockIdx.x;
+    if (r >= num) return;
+    int any = 0;
+    for (int t = threadIdx.x; t < nt && !any; t += blockDim.x) any = tr[(size_t)r * nt + t] != 0.f;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) keep[r] = any;
+}
+
+}  // namespace
+
+int filter_traces(float* d_tr, int nt, int num, const void* d_H, void* d_x, int* d_keep, int ts, void* plan_ptr,
+                  void* stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    cufftHandle plan = *static_cast<cufftHandle*>(plan_ptr);
+    cufftComplex* x = static_cast<cufftComplex*>(d_x);
+    const size_t total = (size_t)ts * num;
+    const int nb = (int)((total + 255) / 256);
+    nonzero_traces<<<num, 256, 0, st>>>(d_tr, nt, num, d_keep);
+    pad_traces<<<nb, 256, 0, st>>>(d_tr, nt, ts, num, x);
+    if (cufftSetStream(plan, st) != CUFFT_SUCCESS) return 1;
+    if (cufftExecC2C(plan, x, x, CUFFT_FORWARD) != CUFFT_SUCCESS) return 2;
+    apply_response<<<nb, 256, 0, st>>>(x, static_cast<const cufftComplex*>(d_H), ts, num, 1.f / float(ts));
+    if (cufftExecC2C(plan, x, x, CUFFT_INVERSE) != CUFFT_SUCCESS) return 3;
+    unpad_traces<<<(int)(((size_t)nt * num + 255) / 256), 256, 0, st>>>(x, nt, ts, num, d_keep, d_tr);
+    return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+int make_fft_plan(int ts, int num, void* plan_out) {
+    cufftHandle plan;
+    int n[1] = {ts};
+    if (cufftPlanMany(&plan, 1, n, nullptr, 1, ts, nullptr, 1, ts, CUFFT_C2C, num) != CUFFT_SUCCESS) return 1;
+    *static_cast<cufftHandle*>(plan_out) = plan;
+    return 0;
+}
+
+void destroy_fft_plan(void* plan) { cufftDestroy(*static_cast<cufftHandle*>(plan)); }
+
+}  // namespace psdm

@@ -2,6 +2,7 @@
 // units of the RTM engine.  Not part of the C ABI.
 #pragma once
 
+#include <complex>
 #include <cstddef>
 #include <cstdint>
 
@@ -150,6 +151,15 @@ struct CondArgs {
     float dt_data, dt_prop;
 };
 int launch_condition(const CondArgs& c, void* stream);
+
+// Frequency filter (rtm_filter.cu): Butterworth response of length ts on the
+// host, and the filtering of num traces of nt samples in place on `stream`
+// with a batched length-ts cuFFT plan (an int handle stored at plan_ptr).
+void butterworth_response(int ts, float fe, int typef, float f1, float fc, std::complex<float>* H);
+int make_fft_plan(int ts, int num, void* plan_out);
+void destroy_fft_plan(void* plan);
+int filter_traces(float* d_tr, int nt, int num, const void* d_H, void* d_x, int* d_keep, int ts, void* plan_ptr,
+                  void* stream);
 
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
 int launch_wait_timeout_probe(int* err, void* stream);

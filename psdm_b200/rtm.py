@@ -208,6 +208,17 @@ class Engine:
         L.check(L.lib().psdm_condition_traces_device(self._h, C.byref(cond), nrec, d_Field_Data, nt_data, dt_data,
                                                      dt_prop, _i32(nt_cut), _i32(nt_sf), _i32(lens), d_Data_target))
 
+    def freq_filter(self, traces, dt, typef, f1, f2):
+        """psdm_freq_filter on a copy of traces (Num, nt); returns the filtered traces."""
+        out = np.array(_f32(traces), dtype=np.float32, copy=True, order="C")
+        num, nt = out.shape
+        L.check(L.lib().psdm_freq_filter(self._h, out.reshape(-1), nt, dt, num, typef, f1, f2))
+        return out
+
+    def freq_filter_device(self, d_traces: int, nt: int, dt: float, num: int, typef: int, f1: float, f2: float):
+        """psdm_freq_filter_device: filters device traces (num, nt) in place (asynchronous)."""
+        L.check(L.lib().psdm_freq_filter_device(self._h, d_traces, nt, dt, num, typef, f1, f2))
+
     def set_checkpointing(self, interval: int):
         """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
         L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))
