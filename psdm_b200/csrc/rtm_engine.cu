@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <complex>
 #include <map>
 #include <string>
@@ -83,7 +84,7 @@ struct psdm_engine {
     bool use_graphs = true;
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
-    std::map<std::pair<int, int>, int> fft_plans;  // (length, batch) -> cuFFT plan handle
+    std::map<std::pair<int, int>, std::array<int, 2>> fft_plans;  // (length, batch) -> cuFFT plans
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
 
@@ -132,7 +133,7 @@ struct psdm_engine {
     }
     int trim() {
         drop_graphs();
-        for (auto& kv : fft_plans) destroy_fft_plan(&kv.second);
+        for (auto& kv : fft_plans) destroy_fft_plans(kv.second.data());
         fft_plans.clear();
         for (auto& kv : bufs)
             if (kv.second.ptr) CUDA_TRY(cudaFree(kv.second.ptr));
@@ -1550,19 +1551,20 @@ int psdm_freq_filter_device(psdm_engine* e, float* d_traces, int32_t nt, float d
     butterworth_response(ts, 1.f / dt, typef, f1, f2, H.data());
     float *d_H = nullptr, *d_x = nullptr;
     int* d_keep = nullptr;
-    TRY(e->get("filt_H", (size_t)ts * 2, &d_H));
-    TRY(e->get("filt_x", (size_t)ts * Num * 2, &d_x));
+    TRY(e->get("filt_H", (size_t)(ts / 2 + 1) * 2, &d_H));
+    TRY(e->get("filt_x", filter_work_floats(ts, Num), &d_x));
     TRY(e->get("filt_keep", (size_t)Num, &d_keep));
-    CUDA_TRY(cudaMemcpyAsync(d_H, H.data(), (size_t)ts * sizeof(std::complex<float>), cudaMemcpyHostToDevice,
-                             e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_H, H.data(), (size_t)(ts / 2 + 1) * sizeof(std::complex<float>),
+                             cudaMemcpyHostToDevice, e->stream));
     auto key = std::make_pair(ts, (int)Num);
     auto it = e->fft_plans.find(key);
     if (it == e->fft_plans.end()) {
-        int plan = 0;
-        if (make_fft_plan(ts, Num, &plan)) return fail(PSDM_ERR_CUDA, "cuFFT plan of length %d x %d failed", ts, Num);
-        it = e->fft_plans.emplace(key, plan).first;
+        std::array<int, 2> plans{};
+        if (make_fft_plans(ts, Num, plans.data()))
+            return fail(PSDM_ERR_CUDA, "cuFFT plans of length %d x %d failed", ts, Num);
+        it = e->fft_plans.emplace(key, plans).first;
     }
-    const int rc = filter_traces(d_traces, nt, Num, d_H, d_x, d_keep, ts, &it->second, e->stream);
+    const int rc = filter_traces(d_traces, nt, Num, d_H, d_x, d_keep, ts, it->second.data(), e->stream);
     if (rc) return fail(PSDM_ERR_CUDA, "frequency filter failed (step %d)", rc);
     e->launches += 5;
     return PSDM_OK;

@@ -4,7 +4,7 @@
 // placed at the end of a zero buffer 24 times its length, transformed,
 // multiplied by the response (and by 1/n, the forward scaling of the
 // reference's FFT), transformed back, and the real part of the last nt
-// samples is kept.  The transforms are cuFFT's (a library FFT, like the
+// samples is kept; see filter_traces for the half-spectrum form used here.  The transforms are cuFFT's (a library FFT, like the
 // reference's vendored FFTPACK); the results agree with the reference's
 // arithmetic to FP32 rounding, not bit for bit.
 
@@ -55,28 +55,31 @@ void butterworth_response(int ts, float fe, int typef, float f1, float fc, std::
 
 namespace {
 
-__global__ void pad_traces(const float* tr, int nt, int ts, int num, cufftComplex* x) {
+// Real input rows of ts samples, the trace at the end of each.
+__global__ void pad_traces(const float* tr, int nt, int ts, int num, float* x) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)ts * num) return;
     const int t = (int)(i % ts), r = (int)(i / ts);
     const int off = ts - nt;
-    x[i] = make_cuComplex(t >= off ? tr[(size_t)r * nt + (t - off)] : 0.f, 0.f);
+    x[i] = t >= off ? tr[(size_t)r * nt + (t - off)] : 0.f;
 }
 
-__global__ void apply_response(cufftComplex* x, const cufftComplex* H, int ts, int num, float scale) {
+// The non-negative half of the spectrum times H / ts (the forward scaling
+// of the reference's transform).
+__global__ void apply_response(cufftComplex* X, const cufftComplex* H, int nh, int num, float scale) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)ts * num) return;
-    const cufftComplex h = H[i % ts], v = x[i];
-    const float re = v.x * scale, im = v.y * scale;  // forward transform scaled by 1/ts
-    x[i] = make_cuComplex(re * h.x - im * h.y, re * h.y + im * h.x);
+    if (i >= (size_t)nh * num) return;
+    const cufftComplex h = H[i % nh], v = X[i];
+    const float re = v.x * scale, im = v.y * scale;
+    X[i] = make_cuComplex(re * h.x - im * h.y, re * h.y + im * h.x);
 }
 
-__global__ void unpad_traces(const cufftComplex* x, int nt, int ts, int num, const int* keep, float* tr) {
+__global__ void unpad_traces(const float* x, int nt, int ts, int num, const int* keep, float* tr) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)nt * num) return;
     const int t = (int)(i % nt), r = (int)(i / nt);
     if (!keep[r]) return;  // an all-zero trace is left as it is (is_not_cero)
-    tr[i] = x[(size_t)r * ts + (ts - nt) + t].x;
+    tr[i] = x[(size_t)r * ts + (ts - nt) + t];
 }
 
 __global__ void nonzero_traces(const float* tr, int nt, int num, int* keep) {
@@ -90,31 +93,52 @@ __global__ void nonzero_traces(const float* tr, int nt, int num, int* keep) {
 
 }  // namespace
 
-int filter_traces(float* d_tr, int nt, int num, const void* d_H, void* d_x, int* d_keep, int ts, void* plan_ptr,
+size_t filter_work_floats(int ts, int num) {
+    const size_t real = ((size_t)ts * num + 3) & ~(size_t)3;  // complex half starts 16-byte aligned
+    return real + (size_t)(ts / 2 + 1) * num * 2;
+}
+
+// The reference transforms the real trace as a complex one and keeps the real
+// part of the inverse.  The product of a real trace's spectrum with the
+// response is Hermitian in every bin but ts/2, where only its real part
+// reaches the real output, so the half-spectrum transforms (real to complex,
+// complex to real, which reads the real part of bin ts/2) give the same
+// result at half the work.
+int filter_traces(float* d_tr, int nt, int num, const void* d_H, float* d_x, int* d_keep, int ts, const int* plans,
                   void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    cufftHandle plan = *static_cast<cufftHandle*>(plan_ptr);
-    cufftComplex* x = static_cast<cufftComplex*>(d_x);
+    const int nh = ts / 2 + 1;
+    float* x = d_x;
+    cufftComplex* X = reinterpret_cast<cufftComplex*>(d_x + (((size_t)ts * num + 3) & ~(size_t)3));
     const size_t total = (size_t)ts * num;
-    const int nb = (int)((total + 255) / 256);
     nonzero_traces<<<num, 256, 0, st>>>(d_tr, nt, num, d_keep);
-    pad_traces<<<nb, 256, 0, st>>>(d_tr, nt, ts, num, x);
-    if (cufftSetStream(plan, st) != CUFFT_SUCCESS) return 1;
-    if (cufftExecC2C(plan, x, x, CUFFT_FORWARD) != CUFFT_SUCCESS) return 2;
-    apply_response<<<nb, 256, 0, st>>>(x, static_cast<const cufftComplex*>(d_H), ts, num, 1.f / float(ts));
-    if (cufftExecC2C(plan, x, x, CUFFT_INVERSE) != CUFFT_SUCCESS) return 3;
+    pad_traces<<<(int)((total + 255) / 256), 256, 0, st>>>(d_tr, nt, ts, num, x);
+    if (cufftSetStream(plans[0], st) != CUFFT_SUCCESS || cufftSetStream(plans[1], st) != CUFFT_SUCCESS) return 1;
+    if (cufftExecR2C(plans[0], x, X) != CUFFT_SUCCESS) return 2;
+    apply_response<<<(int)(((size_t)nh * num + 255) / 256), 256, 0, st>>>(X, static_cast<const cufftComplex*>(d_H), nh,
+                                                                          num, 1.f / float(ts));
+    if (cufftExecC2R(plans[1], X, x) != CUFFT_SUCCESS) return 3;
     unpad_traces<<<(int)(((size_t)nt * num + 255) / 256), 256, 0, st>>>(x, nt, ts, num, d_keep, d_tr);
     return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
 
-int make_fft_plan(int ts, int num, void* plan_out) {
-    cufftHandle plan;
+int make_fft_plans(int ts, int num, int* plans) {
+    cufftHandle a, b;
     int n[1] = {ts};
-    if (cufftPlanMany(&plan, 1, n, nullptr, 1, ts, nullptr, 1, ts, CUFFT_C2C, num) != CUFFT_SUCCESS) return 1;
-    *static_cast<cufftHandle*>(plan_out) = plan;
+    const int nh = ts / 2 + 1;
+    if (cufftPlanMany(&a, 1, n, nullptr, 1, ts, nullptr, 1, nh, CUFFT_R2C, num) != CUFFT_SUCCESS) return 1;
+    if (cufftPlanMany(&b, 1, n, nullptr, 1, nh, nullptr, 1, ts, CUFFT_C2R, num) != CUFFT_SUCCESS) {
+        cufftDestroy(a);
+        return 1;
+    }
+    plans[0] = a;
+    plans[1] = b;
     return 0;
 }
 
-void destroy_fft_plan(void* plan) { cufftDestroy(*static_cast<cufftHandle*>(plan)); }
+void destroy_fft_plans(int* plans) {
+    cufftDestroy(plans[0]);
+    cufftDestroy(plans[1]);
+}
 
 }  // namespace psdm

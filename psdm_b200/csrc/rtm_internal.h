@@ -156,9 +156,10 @@ int launch_condition(const CondArgs& c, void* stream);
 // host, and the filtering of num traces of nt samples in place on `stream`
 // with a batched length-ts cuFFT plan (an int handle stored at plan_ptr).
 void butterworth_response(int ts, float fe, int typef, float f1, float fc, std::complex<float>* H);
-int make_fft_plan(int ts, int num, void* plan_out);
-void destroy_fft_plan(void* plan);
-int filter_traces(float* d_tr, int nt, int num, const void* d_H, void* d_x, int* d_keep, int ts, void* plan_ptr,
+int make_fft_plans(int ts, int num, int* plans);  // plans[0] real-to-complex, plans[1] complex-to-real
+void destroy_fft_plans(int* plans);
+size_t filter_work_floats(int ts, int num);
+int filter_traces(float* d_tr, int nt, int num, const void* d_H, float* d_x, int* d_keep, int ts, const int* plans,
                   void* stream);
 
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.

@@ -868,7 +868,10 @@ __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t*
 // next slot's tiles while others are still waiting for their copies, and a
 // step of many shots fills the GPU in several waves.  Each slot's step
 // arguments live in device memory; a block copies them into shared memory
-// when it switches slot.  Slots may be in different passes (mode 0 / 1).
+// when it switches slot.  Slots may be in different passes (mode 0 / 1 / 2);
+// FIXED >= 0 is the instance for a launch whose slots are all in pass FIXED,
+// compiled without the other passes' code (fewer registers and spills).
+template <int FIXED>
 __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -883,7 +886,7 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
     // Deferred receiver gathers of the forward slots (p = previous step's p3),
     // and their pending snapshot quantizations.
     for (int s = 0; s < bp.nslots; ++s) {
-        if (bp.mode[s] != 0) continue;
+        if (FIXED > 0 || bp.mode[s] != 0) continue;
         const StepArgs* g = bp.args[s];
         const float* qs = g->q_src;
         if (qs != nullptr) quantize_part(qs, g->q_amax, g->q_dst, g->q_iscale, g->q_n, g->kind16, tid);
@@ -926,9 +929,14 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
             cur = s;
         }
         const int lb = b - bp.first[s];
-        const int md = bp.mode[s];
-        const bool ok = md == 0 ? run_tile<0>(sa, sm, &bar, phase, lb)
-                                : (md == 1 ? run_tile<1>(sa, sm, &bar, phase, lb) : run_tile<2>(sa, sm, &bar, phase, lb));
+        bool ok;
+        if (FIXED >= 0) {
+            ok = run_tile<(FIXED >= 0 ? FIXED : 0)>(sa, sm, &bar, phase, lb);
+        } else {
+            const int md = bp.mode[s];
+            ok = md == 0 ? run_tile<0>(sa, sm, &bar, phase, lb)
+                         : (md == 1 ? run_tile<1>(sa, sm, &bar, phase, lb) : run_tile<2>(sa, sm, &bar, phase, lb));
+        }
         if (!ok) return;
         __syncthreads();  // shared tile, tile_id and (next switch) sa are reused
     }
@@ -1050,13 +1058,14 @@ int blocks_per_sm() {
     return nb;
 }
 
+template <int FIXED>
 int batch_blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
         const int bytes = smem_floats<0>() * (int)sizeof(float);
-        cudaFuncSetAttribute(batch_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(batch_step_kernel<FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         int n = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_step_kernel, NT, bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_step_kernel<FIXED>, NT, bytes);
         nb = n > 0 ? n : 1;
     }
     return nb;
@@ -1082,7 +1091,9 @@ int launch_mode(const StepArgs& a, cudaStream_t stream) {
 int prepare_step_kernels() {
     // Kernel attributes and occupancy are set up once, outside any stream
     // capture.
-    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && blocks_per_sm<2>() > 0 && batch_blocks_per_sm() > 0)
+    return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && blocks_per_sm<2>() > 0 &&
+            batch_blocks_per_sm<-1>() > 0 && batch_blocks_per_sm<0>() > 0 && batch_blocks_per_sm<1>() > 0 &&
+            batch_blocks_per_sm<2>() > 0)
                ? (int)cudaGetLastError()
                : 1;
 }
@@ -1107,22 +1118,34 @@ int launch_quantize(const float* src, const unsigned int* amax, void* dst, float
     return (int)cudaGetLastError();
 }
 
-int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
+template <int FIXED>
+int launch_batch(const BatchParams& bp, int num_sms, cudaStream_t stream) {
     const int total = bp.first[bp.nslots];
-    if (bp.nslots <= 0 || total <= 0) return 0;
     const int bytes = smem_floats<0>() * (int)sizeof(float);
-    const dim3 grid(min(total, num_sms * batch_blocks_per_sm()));
+    const dim3 grid(min(total, num_sms * batch_blocks_per_sm<FIXED>()));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(32, NWARP);
     cfg.dynamicSmemBytes = (size_t)bytes;
-    cfg.stream = (cudaStream_t)stream;
+    cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return (int)cudaLaunchKernelEx(&cfg, batch_step_kernel, bp);
+    return (int)cudaLaunchKernelEx(&cfg, batch_step_kernel<FIXED>, bp);
+}
+
+int launch_batch_step(const BatchParams& bp, int num_sms, void* stream) {
+    const int total = bp.first[bp.nslots];
+    if (bp.nslots <= 0 || total <= 0) return 0;
+    bool same = true;
+    for (int s = 1; s < bp.nslots; ++s) same = same && bp.mode[s] == bp.mode[0];
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!same) return launch_batch<-1>(bp, num_sms, st);
+    if (bp.mode[0] == 0) return launch_batch<0>(bp, num_sms, st);
+    if (bp.mode[0] == 1) return launch_batch<1>(bp, num_sms, st);
+    return launch_batch<2>(bp, num_sms, st);
 }
 
 // A bounded wait on copies that are never issued: the mbarrier expects 16
