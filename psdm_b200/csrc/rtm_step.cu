@@ -191,8 +191,10 @@ __device__ __forceinline__ float2 unpack16(unsigned int w, int kind16) {
 }
 
 // Four consecutive snapshot values (16-byte aligned group) as floats.
-__device__ __forceinline__ float4 load16x4(const void* base, int fi, int kind16, float isc) {
-    const uint2 w = __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + fi));
+__device__ __forceinline__ uint2 load16x4_raw(const void* base, int fi) {
+    return __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + fi));
+}
+__device__ __forceinline__ float4 unpack16x4(const uint2 w, int kind16, float isc) {
     const float2 a = unpack16(w.x, kind16), b = unpack16(w.y, kind16);
     return make_float4(__fmul_rn(a.x, isc), __fmul_rn(a.y, isc), __fmul_rn(b.x, isc), __fmul_rn(b.y, isc));
 }
@@ -457,8 +459,9 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi));
         In = *reinterpret_cast<const float4*>(a.image + fi);
     }
+    uint2 Fr = make_uint2(0u, 0u);  // 16-bit snapshot values, converted where used
     if (img16 && active) {
-        Fn = load16x4(a.field16, fi, a.kind16, isc);
+        Fr = load16x4_raw(a.field16, fi);
         In = *reinterpret_cast<const float4*>(a.image + fi);
         Cn = *reinterpret_cast<const float4*>(a.comp + fi);
     }
@@ -502,12 +505,13 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
             c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g + a.ldz));
         }
         float4 Fc = Fn, Ic = In, Cc = Cn;
+        const uint2 Frc = Fr;
         if (img && c + 1 < ncol) {  // next column of the snapshot and image
             Fn = __ldg(reinterpret_cast<const float4*>(a.field + fi + a.ldf));
             In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
         }
         if (img16 && c + 1 < ncol) {
-            Fn = load16x4(a.field16, fi + a.ldf, a.kind16, isc);
+            Fr = load16x4_raw(a.field16, fi + a.ldf);
             In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
             Cn = *reinterpret_cast<const float4*>(a.comp + fi + a.ldf);
         }
@@ -563,6 +567,7 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
                 amax_t = fmaxf(amax_t, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(sv.z), fabsf(sv.w))));
         }
         if (MODE == 2 && img16) {
+            Fc = unpack16x4(Frc, a.kind16, isc);
             float Fv[4] = {Fc.x, Fc.y, Fc.z, Fc.w};
             float Iv[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
             float Cv[4] = {Cc.x, Cc.y, Cc.z, Cc.w};
