@@ -433,7 +433,7 @@ int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args) {
 //   receiver cells; the per-step arguments are appended to *steps_out.
 int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
                   float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec, const std::string& tag,
-                  std::vector<StepArgs>* steps_out) {
+                  std::vector<StepArgs>* steps_out, bool batched = false) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, 1, &zs, &xs, &inj));
@@ -446,7 +446,7 @@ int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* 
         CUDA_TRY(cudaMemsetAsync(d_rec, 0, (size_t)nrec * nt * sizeof(float), e->stream));
     }
     StepArgs a = base_args(s);
-    plan_tiles(&a, inj.row_slot.data());
+    plan_tiles(&a, inj.row_slot.data(), batched);
     a.row_slot = d_row;
     a.inj_cols = d_cols;
     a.inj_trace = d_S;
@@ -505,14 +505,14 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
 int build_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
                    int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
                    const float* h_w, float* d_image, const std::string& tag, std::vector<StepArgs>* steps_out,
-                   std::vector<int>* slot_of_step = nullptr) {
+                   std::vector<int>* slot_of_step = nullptr, bool batched = false) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, nrec, zr, xr, &inj));
     int *d_row = nullptr, *d_cols = nullptr;
     TRY(upload_inj(e, g, inj, ("rec" + tag).c_str(), &d_row, &d_cols));
     StepArgs a = base_args(s);
-    plan_tiles(&a, inj.row_slot.data());
+    plan_tiles(&a, inj.row_slot.data(), batched);
     a.row_slot = d_row;
     a.inj_cols = d_cols;
     a.inj_trace = d_back;
@@ -1020,12 +1020,12 @@ int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
     const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, j.taper_option, j.N_taper, j.N_zeros);
     std::vector<StepArgs> steps;
     TRY(build_forward(e, sl.s, nt_prop2, j.store_snap, j.d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr, tag,
-                      &steps));
+                      &steps, true));
     sl.nfwd = (int)steps.size();
     sl.pending = 0;
     if (mixed) mixed_forward_args(sl.mb, steps, 0, &sl.pending);
     TRY(build_backward(e, sl.s, nt_taper, j.store_snap, nt_taper, d_tgt, 1, sh.NumRec, w.zr.data(), w.xr.data(),
-                       d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps));
+                       d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps, nullptr, true));
     if (mixed) mixed_backward_args(sl.mb, nt_taper, wts.data(), steps, (size_t)sl.nfwd);
     sl.bwd_mode = mixed ? 2 : 1;
     sl.nbwd = (int)steps.size() - sl.nfwd;

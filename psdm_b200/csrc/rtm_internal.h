@@ -85,6 +85,7 @@ struct StepArgs {
     // [r_zd0, r_zd0+r_h) x columns [r_x0, r_x0+r_w); its tiles are blocks
     // [r_first[r], r_first[r+1]) with r_tz tiles along z.
     int nrect;
+    int itx;  // interior tile columns the plan was made for (one-shot or batched launches)
     int r_type[16], r_zd0[16], r_x0[16], r_h[16], r_w[16], r_tz[16], r_first[17];
     // persistent scheduling: tile_counter[counter_sel] starts at 0 (cleared
     // by the previous step); num_sms = multiprocessor count of the device
@@ -126,8 +127,9 @@ struct BatchParams {
 
 // Fill the block decomposition of `a` from its grid fields (nyt, nxt, ny,
 // nx, dn, zoff, fs) and the host copy of the injection row map (ldz
-// entries, or null when nothing is injected).
-void plan_tiles(StepArgs* a, const int* row_slot_host);
+// entries, or null when nothing is injected).  `batched` plans the interior
+// tiles of batch_step_kernel, otherwise those of step_kernel.
+void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched = false);
 
 // Set kernel attributes (shared memory carve-out, occupancy); call once per
 // device before the first launch.  Returns a cudaError_t value.

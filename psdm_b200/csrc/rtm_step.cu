@@ -51,15 +51,19 @@
 namespace psdm {
 namespace {
 
-// Interior tiles: 128 rows x 32 columns, each thread 4 rows x 8 columns.
+// Interior tiles: 128 rows x (4 XS) columns, each thread 4 rows x XS
+// columns.  A launch of one shot has fewer tiles than resident blocks and
+// gains from narrower tiles (more of them in flight); a batched launch runs
+// several waves and gains from wider ones (less halo per cell).
 constexpr int QZ = 32;          // float4 rows per interior tile (one warp along z)
 constexpr int TZ = 4 * QZ;      // interior tile rows
 constexpr int NWARP = 4;        // warps per block
-constexpr int XS = 8;           // columns per thread (interior)
-constexpr int TX = NWARP * XS;  // interior tile columns
+constexpr int XS_ONE = 7;       // columns per thread, one shot per launch
+constexpr int XS_MANY = 8;      // columns per thread, batched launches
 constexpr int HZ = TZ + 8;      // shared rows (16-byte aligned halo of >= 3)
 constexpr int HQ = HZ / 4;      // shared float4 rows
-constexpr int WX = TX + 6;      // shared columns (halo of 3)
+__host__ __device__ constexpr int tile_cols(int xs) { return NWARP * xs; }      // interior tile columns
+__host__ __device__ constexpr int tile_smem_cols(int xs) { return NWARP * xs + 6; }  // with a 3-column halo
 // C-PML / boundary tiles: 32 rows x 16 columns, each thread 1 row x 4 columns.
 constexpr int PTZ = 32;
 constexpr int PXS = 4;
@@ -425,10 +429,15 @@ __device__ __forceinline__ float2 add_prod(const float2& a, const float2& b) {
     return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
 }
 
-template <int MODE>
+template <int MODE, int XS>
 __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int r,
                                               int t) {
+    constexpr int TX = tile_cols(XS);
     const int lane = threadIdx.x, wy = threadIdx.y;
+    if (a.itx != TX) {  // planned for the other tile width: report, touch nothing
+        if (lane == 0 && wy == 0) atomicExch(a.err, 2);
+        return false;
+    }
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
     const int z0 = a.r_zd0[r] + tz * TZ, x0 = a.r_x0[r] + tx * TX;
     const int nrows = min(TZ, a.r_zd0[r] + a.r_h[r] - z0);  // a multiple of 4
@@ -798,9 +807,9 @@ __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r
     }
 }
 
-template <int MODE>
+template <int XS>
 constexpr int smem_floats() {
-    return WX * HZ;  // the p tile of an interior tile (boundary tiles use less)
+    return tile_smem_cols(XS) * HZ;  // the p tile of an interior tile (boundary tiles use less)
 }
 
 template <int MODE>
@@ -840,7 +849,7 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
         const int t = b - a.r_first[r];
         switch (a.r_type[r]) {
             case 0:
-                if (!interior_tile<MODE>(a, sm, &bar, phase, r, t)) return;
+                if (!interior_tile<MODE, XS_ONE>(a, sm, &bar, phase, r, t)) return;
                 break;
             case 1: xband_tile<MODE>(a, sm, r, t); break;
             case 2: zstrip_tile<MODE>(a, sm, r, t); break;
@@ -859,7 +868,7 @@ __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t*
     while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
     const int t = b - a.r_first[r];
     switch (a.r_type[r]) {
-        case 0: return interior_tile<MODE>(a, sm, bar, phase, r, t);
+        case 0: return interior_tile<MODE, XS_MANY>(a, sm, bar, phase, r, t);
         case 1: xband_tile<MODE>(a, sm, r, t); return true;
         case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
         case 4: rowband_tile<MODE>(a, sm, r, t); return true;
@@ -979,7 +988,9 @@ __global__ void pad_c2_kernel(const float* vp, int ny, int nx, int dn, int nyt, 
 
 }  // namespace
 
-void plan_tiles(StepArgs* a, const int* row_slot_host) {
+void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched) {
+    const int TX = tile_cols(batched ? XS_MANY : XS_ONE);
+    a->itx = TX;
     // Rects of the padded grid (device rows), heaviest first:
     //   type 0  interior band rows without injection / free surface
     //   type 1  x-strip band   rows [d0, d0+ny4) x C-PML columns
@@ -1054,7 +1065,7 @@ template <int MODE>
 int blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
-        const int bytes = smem_floats<MODE>() * (int)sizeof(float);
+        const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
         cudaFuncSetAttribute(step_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<MODE>, NT, bytes);
@@ -1067,7 +1078,7 @@ template <int FIXED>
 int batch_blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
-        const int bytes = smem_floats<0>() * (int)sizeof(float);
+        const int bytes = smem_floats<XS_MANY>() * (int)sizeof(float);
         cudaFuncSetAttribute(batch_step_kernel<FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_step_kernel<FIXED>, NT, bytes);
@@ -1078,7 +1089,7 @@ int batch_blocks_per_sm() {
 
 template <int MODE>
 int launch_mode(const StepArgs& a, cudaStream_t stream) {
-    const int bytes = smem_floats<MODE>() * (int)sizeof(float);
+    const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
     const dim3 grid(min(a.r_first[a.nrect], a.num_sms * blocks_per_sm<MODE>()));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -1126,7 +1137,7 @@ int launch_quantize(const float* src, const unsigned int* amax, void* dst, float
 template <int FIXED>
 int launch_batch(const BatchParams& bp, int num_sms, cudaStream_t stream) {
     const int total = bp.first[bp.nslots];
-    const int bytes = smem_floats<0>() * (int)sizeof(float);
+    const int bytes = smem_floats<XS_MANY>() * (int)sizeof(float);
     const dim3 grid(min(total, num_sms * batch_blocks_per_sm<FIXED>()));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
