@@ -196,6 +196,15 @@ int psdm_rtm_batch_device(
  * the batched or mixed-precision forms.
  */
 int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval);
+/*
+ * Launch form of one shot's passes (psdm_rtm_shot, psdm_model_shot and their
+ * device variants): 1 runs a pass whose steps allow it as one cooperative
+ * launch in which each tile advances as soon as its neighbours finished the
+ * previous step; 0 (default) launches one kernel per time step (replayed
+ * from a CUDA graph).  Same results bit for bit.  Passes with the
+ * mixed-precision snapshot conversion always use one launch per step.
+ */
+int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on);
 
 /* Shots in flight at a time in the last batched call. */
 int32_t psdm_engine_batch_slots(const psdm_engine* e);

@@ -82,6 +82,12 @@ struct psdm_engine {
         cudaGraphExec_t exec = nullptr;
     } graphs[3];
     bool use_graphs = true;
+    // Passes of one shot as one cooperative launch each (pass_kernel) where
+    // the pass allows it; the neighbour and receiver lists of the last plan
+    // of each pass kind stay on the device while the plan (key) is unchanged.
+    bool use_pass = false;
+    std::vector<int> pass_key[3];  // by pass kind (mode)
+    cudaEvent_t pass_staged[3] = {nullptr, nullptr, nullptr};  // copies out of the staging buffers done
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
     std::map<std::pair<int, int>, std::array<int, 2>> fft_plans;  // (length, batch) -> cuFFT plans
@@ -133,6 +139,7 @@ struct psdm_engine {
     }
     int trim() {
         drop_graphs();
+        for (auto& k : pass_key) k.clear();
         for (auto& kv : fft_plans) destroy_fft_plans(kv.second.data());
         fft_plans.clear();
         for (auto& kv : bufs)
@@ -380,13 +387,180 @@ void set_buffers(const Shot& s, int it, StepArgs* a) {
     a->side_pm = s.side[c ^ 1];
 }
 
+// The steps of a pass as the pass kernel's input: the arguments of the first
+// two steps as parity bases, and the values that change from step to step.
+// False when steps differ in anything else, or when a step reduces over the
+// whole grid (the mixed form's per-snapshot maximum and its conversion), which
+// the pass kernel's tile-by-tile progress cannot order.
+bool pass_form(const std::vector<StepArgs>& args, StepArgs base[2], std::vector<PassVar>* var) {
+    const size_t n = args.size();
+    base[0] = args[0];
+    base[1] = n > 1 ? args[1] : args[0];
+    var->assign(n, PassVar{});
+    for (size_t i = 0; i < n; ++i) {
+        const StepArgs& a = args[i];
+        if (a.q_src != nullptr || a.field_amax != nullptr) return false;
+        if (a.counter_sel != (int)(i & 1)) return false;
+        PassVar& v = (*var)[i];
+        v.field = a.field;
+        v.field16 = a.field16;
+        v.field_iscale = a.field_iscale;
+        v.field_w = a.field_w;
+        v.inj_t = a.inj_t;
+        v.rec_t = a.rec_t;
+        v.par = (int)(i & 1);
+        const StepArgs& b = base[i & 1];
+        StepArgs t = a;
+        t.field = b.field;
+        t.field16 = b.field16;
+        t.field_iscale = b.field_iscale;
+        t.field_w = b.field_w;
+        t.inj_t = b.inj_t;
+        t.rec_t = b.rec_t;
+        if (std::memcmp(&t, &b, sizeof(StepArgs)) != 0) return false;
+    }
+    const StepArgs &b0 = base[0], &b1 = base[1];
+    return b0.nrect == b1.nrect && b0.itx == b1.itx && std::memcmp(b0.r_type, b1.r_type, sizeof b0.r_type) == 0 &&
+           std::memcmp(b0.r_zd0, b1.r_zd0, sizeof b0.r_zd0) == 0 && std::memcmp(b0.r_x0, b1.r_x0, sizeof b0.r_x0) == 0 &&
+           std::memcmp(b0.r_h, b1.r_h, sizeof b0.r_h) == 0 && std::memcmp(b0.r_w, b1.r_w, sizeof b0.r_w) == 0 &&
+           std::memcmp(b0.r_tz, b1.r_tz, sizeof b0.r_tz) == 0 &&
+           std::memcmp(b0.r_first, b1.r_first, sizeof b0.r_first) == 0;
+}
+
+// Neighbour lists of a plan (tiles within kTileReadHalo cells of each other,
+// the reach of every tile's reads) and the receivers held by each tile, both
+// as offset arrays.
+void pass_lists(const StepArgs& a, int nrec, const int* h_rec_cell, std::vector<int>* nbr_first,
+                std::vector<int>* nbr, std::vector<int>* rec_first, std::vector<int>* rec_idx) {
+    const int n = a.r_first[a.nrect];
+    std::vector<std::array<int, 4>> R(n);
+    for (int b = 0; b < n; ++b) tile_rect(a, b, &R[b][0], &R[b][1], &R[b][2], &R[b][3]);
+    const int H = kTileReadHalo;
+    nbr_first->assign(n + 1, 0);
+    nbr->clear();
+    for (int b = 0; b < n; ++b) {
+        for (int c = 0; c < n; ++c)
+            if (c != b && R[c][0] < R[b][1] + H && R[b][0] - H < R[c][1] && R[c][2] < R[b][3] + H &&
+                R[b][2] - H < R[c][3])
+                nbr->push_back(c);
+        (*nbr_first)[b + 1] = (int)nbr->size();
+    }
+    // A cell in no tile is never updated: its p stays 0, as the zeroed traces
+    // already hold.
+    std::vector<std::vector<int>> by(n);
+    for (int i = 0; i < nrec; ++i) {
+        const int x = h_rec_cell[i] / a.ldz, zd = h_rec_cell[i] % a.ldz;
+        for (int b = 0; b < n; ++b)
+            if (zd >= R[b][0] && zd < R[b][1] && x >= R[b][2] && x < R[b][3]) {
+                by[b].push_back(i);
+                break;
+            }
+    }
+    rec_first->assign(n + 1, 0);
+    rec_idx->clear();
+    for (int b = 0; b < n; ++b) {
+        rec_idx->insert(rec_idx->end(), by[b].begin(), by[b].end());
+        (*rec_first)[b + 1] = (int)rec_idx->size();
+    }
+}
+
+// One cooperative launch for the whole pass.  Returns PSDM_OK when launched,
+// 1 when the pass does not have the form (the caller launches per step), or
+// an error code.
+int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args, int nrec, const int* h_rec_cell) {
+    StepArgs base[2];
+    std::vector<PassVar> var;
+    if (!pass_form(args, base, &var)) return 1;
+    const StepArgs& a = base[0];
+    if (mode == 0 && a.nrec > 0 && (h_rec_cell == nullptr || nrec != a.nrec)) return 1;
+    const int ntiles = a.r_first[a.nrect];
+    const int nb = pass_blocks_per_sm(mode);
+    if (nb <= 0 || ntiles <= 0) return 1;
+    const int grid = std::min(ntiles, nb * e->num_sms);
+    std::vector<int> key = {mode == 0 ? a.nrec : 0, a.nrect, a.itx, a.ldz, a.nxt};
+    key.insert(key.end(), a.r_type, a.r_type + a.nrect);
+    key.insert(key.end(), a.r_zd0, a.r_zd0 + a.nrect);
+    key.insert(key.end(), a.r_x0, a.r_x0 + a.nrect);
+    key.insert(key.end(), a.r_h, a.r_h + a.nrect);
+    key.insert(key.end(), a.r_w, a.r_w + a.nrect);
+    if (mode == 0 && a.nrec > 0) key.insert(key.end(), h_rec_cell, h_rec_cell + nrec);
+    int *d_nf = nullptr, *d_nb = nullptr, *d_rf = nullptr, *d_ri = nullptr;
+    const std::string m = std::to_string(mode);
+    const bool fresh = key != e->pass_key[mode];
+    std::vector<int> nf, nbv, rf, ri;
+    if (fresh) {
+        pass_lists(a, mode == 0 ? a.nrec : 0, h_rec_cell, &nf, &nbv, &rf, &ri);
+        e->pass_key[mode].clear();
+    }
+    TRY(e->get(("pass_nbr_first" + m).c_str(), nf.size(), &d_nf));
+    TRY(e->get(("pass_nbr" + m).c_str(), std::max<size_t>(nbv.size(), 1), &d_nb));
+    TRY(e->get(("pass_rec_first" + m).c_str(), rf.size(), &d_rf));
+    TRY(e->get(("pass_rec_idx" + m).c_str(), std::max<size_t>(ri.size(), 1), &d_ri));
+    if (fresh) {
+        CUDA_TRY(cudaMemcpyAsync(d_nf, nf.data(), nf.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        if (!nbv.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_nb, nbv.data(), nbv.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_rf, rf.data(), rf.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        if (!ri.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_ri, ri.data(), ri.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));  // the host lists go out of scope
+        e->pass_key[mode] = key;
+    }
+    StepArgs* d_base = nullptr;
+    PassVar* d_var = nullptr;
+    int* d_flags = nullptr;
+    TRY(e->get(("pass_base" + m).c_str(), 2, &d_base));
+    TRY(e->get(("pass_var" + m).c_str(), var.size(), &d_var));
+    TRY(e->get("pass_flags", (size_t)ntiles, &d_flags));
+    // Staged through page-locked buffers, one per pass kind, refilled only
+    // after the previous copy out of them has completed.
+    const size_t sbytes = 2 * sizeof(StepArgs) + var.size() * sizeof(PassVar);
+    char* h = nullptr;
+    const std::string sname = "pass_stage" + m;
+    TRY(e->get_pinned(sname.c_str(), sbytes, reinterpret_cast<void**>(&h)));
+    cudaEvent_t& done = e->pass_staged[mode];
+    if (done == nullptr) CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventSynchronize(done));
+    std::memcpy(h, base, 2 * sizeof(StepArgs));
+    std::memcpy(h + 2 * sizeof(StepArgs), var.data(), var.size() * sizeof(PassVar));
+    CUDA_TRY(cudaMemcpyAsync(d_base, h, 2 * sizeof(StepArgs), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_var, h + 2 * sizeof(StepArgs), var.size() * sizeof(PassVar), cudaMemcpyHostToDevice,
+                             e->stream));
+    CUDA_TRY(cudaEventRecord(done, e->stream));
+    CUDA_TRY(cudaMemsetAsync(d_flags, 0, (size_t)ntiles * sizeof(int), e->stream));
+    PassParams pp{};
+    pp.base = d_base;
+    pp.var = d_var;
+    pp.nsteps = (int)var.size();
+    pp.ntiles = ntiles;
+    pp.nbr_first = d_nf;
+    pp.nbr = d_nb;
+    pp.rec_first = d_rf;
+    pp.rec_idx = d_ri;
+    pp.flags = d_flags;
+    pp.err = a.err;
+    const int rc = launch_pass(mode, pp, grid, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "pass launch: %s", cudaGetErrorString((cudaError_t)rc));
+    return PSDM_OK;
+}
+
 // Launch the step kernels of one pass.  The launches are captured once into
 // a CUDA graph and the graph is replayed while the argument list is
 // identical (same buffers, geometry, step count and per-step values), which
 // removes the host launch cost per time step.  Falls back to direct launches
 // if the capture is not possible.
-int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args) {
+int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args, int nrec = 0,
+                 const int* h_rec_cell = nullptr) {
     if (args.empty()) return PSDM_OK;
+    if (e->use_pass) {
+        const int rc = launch_pass_form(e, mode, args, nrec, h_rec_cell);
+        if (rc == PSDM_OK) {
+            e->launches += 1;
+            return PSDM_OK;
+        }
+        if (rc != 1) return rc;
+    }
+    e->launches += (int64_t)args.size();
     auto& gc = e->graphs[mode];
     if (e->use_graphs) {
         const bool same = gc.exec && gc.args.size() == args.size() &&
@@ -482,8 +656,7 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
     std::vector<StepArgs> steps;
     TRY(build_forward(e, s, nt, store_snap, d_S, zs, xs, d_fields, nslots, nrec, h_rec_cell, d_rec, "", &steps));
     const int* d_rec_cell = steps.empty() ? nullptr : steps[0].rec_cell;
-    TRY(launch_steps(e, 0, steps));
-    e->launches += nt - 1;
+    TRY(launch_steps(e, 0, steps, nrec, h_rec_cell));
     e->fwd_steps += nt - 1;
     if (d_rec && nrec > 0 && nt >= 2) {
         const float* pfin = s.p[(nt - 1) & 1];  // p3 of the last step
@@ -552,7 +725,6 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
     TRY(build_backward(e, s, nt, store_snap, nt_snap, d_back, reverse, nrec, zr, xr, d_fields, slot_lo, slot_hi, h_w,
                        d_image, "", &steps));
     TRY(launch_steps(e, 1, steps));
-    e->launches += nt - 1;
     e->bwd_steps += nt - 1;
     return PSDM_OK;
 }
@@ -566,7 +738,10 @@ int check_engine(psdm_engine* e) {
 int sync(psdm_engine* e) {
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     if (e->h_err && *e->h_err) {
+        const int code = *e->h_err;
         *e->h_err = 0;
+        if (code == 2) return fail(PSDM_ERR_CUDA, "a step kernel was given a tile plan for another launch form");
+        if (code == 3) return fail(PSDM_ERR_CUDA, "a pass kernel timed out waiting for neighbouring tiles");
         return fail(PSDM_ERR_CUDA, "a step kernel timed out waiting for its shared-memory copies");
     }
     return PSDM_OK;
@@ -876,7 +1051,6 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
         int pending = 0;
         mixed_forward_args(mb, fw, 0, &pending);
         TRY(launch_steps(e, 0, fw));
-        e->launches += nt_prop2 - 1;
         e->fwd_steps += nt_prop2 - 1;
         TRY(mixed_quantize(e, mb, pending));
         TRY(e->record(1));
@@ -888,7 +1062,6 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
                            1, 0, nullptr, d_imgp, "", &bw));
         mixed_backward_args(mb, nt_taper, wts.data(), bw, 0);
         TRY(launch_steps(e, 2, bw));
-        e->launches += nt_taper - 1;
         e->bwd_steps += nt_taper - 1;
         TRY(e->record(2));
         CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
@@ -1245,6 +1418,8 @@ int psdm_engine_destroy(psdm_engine* e) {
     cudaStreamSynchronize(e->stream);
     int rc = e->trim();
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : e->pass_staged)
+        if (ev) cudaEventDestroy(ev);
     if (e->h_err) cudaFreeHost((void*)e->h_err);
     cudaStreamDestroy(e->own_stream);
     delete e;
@@ -1469,6 +1644,12 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
 }
 
 int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
+
+int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on) {
+    TRY(check_engine(e));
+    e->use_pass = on != 0;
+    return PSDM_OK;
+}
 
 int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval) {
     TRY(check_engine(e));

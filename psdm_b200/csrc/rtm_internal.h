@@ -164,6 +164,47 @@ size_t filter_work_floats(int ts, int num);
 int filter_traces(float* d_tr, int nt, int num, const void* d_H, float* d_x, int* d_keep, int ts, const int* plans,
                   void* stream);
 
+// ---- One launch per pass (dataflow form) --------------------------------
+// A pass of one shot as a single cooperative launch: every tile of the plan
+// is owned by one resident block, which advances it step after step as soon
+// as the tiles whose cells its stencils read (its neighbours) have finished
+// the previous step.  Tiles publish their completed step count in `flags`;
+// waits are bounded and report through err.  Step arguments are the two
+// parity bases with the per-step values of PassVar patched in.
+struct PassVar {
+    float* field;
+    const void* field16;
+    const float* field_iscale;
+    float field_w;
+    int inj_t;
+    int rec_t;
+    int par;
+    int pad_;
+};
+static_assert(sizeof(PassVar) % 16 == 0, "PassVar is fetched in 16-byte pieces");
+
+struct PassParams {
+    const StepArgs* base;  // [2], by step parity
+    const PassVar* var;    // [nsteps]
+    int nsteps;
+    int ntiles;
+    const int* nbr_first;  // [ntiles + 1]
+    const int* nbr;        // neighbour tiles of each tile
+    const int* rec_first;  // [ntiles + 1]
+    const int* rec_idx;    // receivers whose cell lies in each tile
+    int* flags;            // [ntiles] steps completed, zero at launch
+    int* err;
+};
+
+// Cell rectangle [z0, z1) x [x0, x1) (device rows, columns) of tile b of a plan.
+void tile_rect(const StepArgs& a, int b, int* z0, int* z1, int* x0, int* x1);
+// Halo (cells) within which a tile's reads of p, phi and the snapshot lie.
+constexpr int kTileReadHalo = 12;
+// Resident blocks per multiprocessor of the pass kernel (0 on failure).
+int pass_blocks_per_sm(int mode);
+// Launch one pass (modes 0, 1, 2) with `grid` co-resident blocks.
+int launch_pass(int mode, const PassParams& pp, int grid, void* stream);
+
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
 int launch_wait_timeout_probe(int* err, void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.

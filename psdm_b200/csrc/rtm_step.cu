@@ -272,7 +272,7 @@ __device__ __forceinline__ void load_tile_from(const float* src, const StepArgs&
         const int gx = sx0 + col, gz = sz0 + 4 * r4;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (gx >= 0 && gx < a.nxt && gz >= 0 && gz < a.ldz)
-            v = __ldg(reinterpret_cast<const float4*>(src + gx * a.ldz + gz));
+            v = *reinterpret_cast<const float4*>(src + gx * a.ldz + gz);
         *reinterpret_cast<float4*>(&ps[col * (4 * hq) + 4 * r4]) = v;
     }
 }
@@ -322,7 +322,7 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
             const int sb = (x < dn) ? 0 : dn + a.nx;
             const int ci = clampi(x - sb, 3, dn - 4) + sb;
             const float* ph = a.phix_in + ci * a.ldz + zd;
-#define PX(k) __ldg(ph + (k) * a.ldz)
+#define PX(k) ph[(k) * a.ldz]
             const float dph = D1(PX, a.cf1);
 #undef PX
             const float phn = __fadd_rn(__fmul_rn(A, a.phix_in[g]), __fmul_rn(B, d1));
@@ -336,7 +336,7 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
             const int sb = (z < dn) ? 0 : dn + a.ny;
             const int cj = clampi(z - sb, 3, dn - 4) + sb + a.zoff;
             const float* ph = a.phiz_in + x * a.ldz + cj;
-#define PZ(k) __ldg(ph + (k))
+#define PZ(k) ph[(k)]
             const float dph = D1(PZ, a.cf1);
 #undef PZ
             const float phn = __fadd_rn(__fmul_rn(A, a.phiz_in[g]), __fmul_rn(B, d1));
@@ -680,9 +680,9 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
         float4 F[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k)
-            if (k != 3) F[k] = __ldg(reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd));
+            if (k != 3) F[k] = *reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd);
         F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 phc = __ldg(reinterpret_cast<const float4*>(a.phix_in + g));
+        const float4 phc = *reinterpret_cast<const float4*>(a.phix_in + g);
         const float4 chc = *reinterpret_cast<const float4*>(a.chix + g);
         const float4 pmv = *reinterpret_cast<const float4*>(a.pm + g);
         const float4 c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
@@ -769,11 +769,11 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
 #undef AX
         const int g = x * a.ldz + zd;
         const float* phs = a.phiz_in + x * a.ldz;
-#define PZ(k) __ldg(phs + cj + (k))
+#define PZ(k) phs[cj + (k)]
         const float dph = D1(PZ, c1);
 #undef PZ
 #undef AZ
-        const float phn = __fadd_rn(__fmul_rn(A, __ldg(phs + zd)), __fmul_rn(B, d1));
+        const float phn = __fadd_rn(__fmul_rn(A, phs[zd]), __fmul_rn(B, d1));
         const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
         a.phiz_out[g] = phn;
         a.chiz[g] = chn;
@@ -862,13 +862,13 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
 
 // One tile (block-local index b of the step described by `a`).  Returns
 // false if its bulk copies did not complete.
-template <int MODE>
+template <int MODE, int XS = XS_MANY>
 __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int b) {
     int r = 0;
     while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
     const int t = b - a.r_first[r];
     switch (a.r_type[r]) {
-        case 0: return interior_tile<MODE, XS_MANY>(a, sm, bar, phase, r, t);
+        case 0: return interior_tile<MODE, XS>(a, sm, bar, phase, r, t);
         case 1: xband_tile<MODE>(a, sm, r, t); return true;
         case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
         case 4: rowband_tile<MODE>(a, sm, r, t); return true;
@@ -953,6 +953,125 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
         }
         if (!ok) return;
         __syncthreads();  // shared tile, tile_id and (next switch) sa are reused
+    }
+}
+
+// ---- one launch per pass (dataflow form)
+
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// Later bulk copies (async proxy) of this thread see what its generic-proxy
+// acquire made visible.
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Wait until *flag >= need: relaxed polls, then one acquire fence.  Gives up
+// after ~1 s, or at once when another block has reported an error.
+__device__ bool wait_flag(const int* flag, int need, const int* err) {
+    if (ld_relaxed(flag) < need) {
+        const uint64_t t0 = globaltimer_ns();
+        for (int it = 0;; ++it) {
+            if (ld_relaxed(flag) >= need) break;
+            if (it >= 32) __nanosleep(64);
+            if ((it & 15) == 15 && (ld_relaxed(err) != 0 || globaltimer_ns() - t0 > 1000000000ull)) return false;
+        }
+    }
+    fence_acq_rel_gpu();
+    return true;
+}
+
+// All steps of one pass.  Block b owns tiles b, b + gridDim.x, ...; before
+// step i of a tile it waits until each neighbour tile has completed i steps
+// (the neighbours wrote the p, phi and side values this step reads, and
+// have read the values this step overwrites), and after it publishes i + 1.
+// Receivers are gathered at the start of a step by the owner of their cell,
+// from p = the previous step's p3, like step_kernel does.  All blocks must be
+// resident at once (cooperative launch).
+template <int MODE>
+__global__ void __launch_bounds__(NT, 5) pass_kernel(const PassParams pp) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(16) StepArgs sb[2];
+    __shared__ __align__(16) PassVar sv[2];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    constexpr int kWords = (int)(sizeof(StepArgs) / sizeof(long long));
+    constexpr int kVar16 = (int)(sizeof(PassVar) / 16);
+    if (tid == 0) mbar_init(&bar, 1);
+    for (int w = tid; w < 2 * kWords; w += NT)
+        reinterpret_cast<long long*>(sb)[w] = reinterpret_cast<const long long*>(pp.base)[w];
+    if (tid == 0 && pp.nsteps > 0) {
+        for (int q = 0; q < kVar16; ++q)
+            cp_async16(reinterpret_cast<char*>(&sv[0]) + 16 * q, reinterpret_cast<const char*>(pp.var) + 16 * q);
+        cp_async_commit();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (int i = 0; i < pp.nsteps; ++i) {
+        const int par = i & 1;
+        if (tid == 0) {
+            cp_async_wait_all();  // values of step i
+            const PassVar& v = sv[par];
+            StepArgs& t = sb[par];
+            t.field = v.field;
+            t.field16 = v.field16;
+            t.field_iscale = v.field_iscale;
+            t.field_w = v.field_w;
+            t.inj_t = v.inj_t;
+            t.rec_t = v.rec_t;
+            if (i + 1 < pp.nsteps) {
+                const char* src = reinterpret_cast<const char*>(pp.var + i + 1);
+                for (int q = 0; q < kVar16; ++q)
+                    cp_async16(reinterpret_cast<char*>(&sv[par ^ 1]) + 16 * q, src + 16 * q);
+                cp_async_commit();
+            }
+        }
+        __syncthreads();
+        const StepArgs& a = sb[par];
+        if (MODE == 0 && a.rec_t >= 0) {  // own cells, written by this block in the previous step
+            for (int T = blockIdx.x; T < pp.ntiles; T += gridDim.x)
+                for (int j = pp.rec_first[T] + tid; j < pp.rec_first[T + 1]; j += NT) {
+                    const int r = pp.rec_idx[j];
+                    a.rec_out[(size_t)r * a.rec_ld + a.rec_t] = a.p[a.rec_cell[r]];
+                }
+        }
+        for (int T = blockIdx.x; T < pp.ntiles; T += gridDim.x) {
+            bool ok = true;
+            for (int k = pp.nbr_first[T] + tid; k < pp.nbr_first[T + 1]; k += NT)
+                ok = wait_flag(pp.flags + pp.nbr[k], i, pp.err) && ok;
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) {
+                    atomicCAS(pp.err, 0, 3);
+                    cp_async_wait_all();
+                }
+                return;
+            }
+            fence_proxy_async_global();
+            if (!run_tile<MODE, XS_ONE>(a, sm, &bar, phase, T)) {
+                if (tid == 0) {
+                    atomicCAS(pp.err, 0, 1);
+                    cp_async_wait_all();
+                }
+                return;
+            }
+            __syncthreads();  // the tile's writes precede the publication; shared tile reused
+            if (tid == 0) {
+                __threadfence();
+                st_release(pp.flags + T, i + 1);
+            }
+        }
     }
 }
 
@@ -1104,14 +1223,70 @@ int launch_mode(const StepArgs& a, cudaStream_t stream) {
     return (int)cudaLaunchKernelEx(&cfg, step_kernel<MODE>, a);
 }
 
+template <int MODE>
+int pass_blocks_per_sm_t() {
+    static int nb = -1;
+    if (nb < 0) {
+        const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
+        cudaFuncSetAttribute(pass_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pass_kernel<MODE>, NT, bytes) != cudaSuccess) n = 0;
+        nb = n;
+    }
+    return nb;
+}
+
+template <int MODE>
+int launch_pass_t(const PassParams& pp, int grid, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(32, NWARP);
+    cfg.dynamicSmemBytes = (size_t)smem_floats<XS_ONE>() * sizeof(float);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, pass_kernel<MODE>, pp);
+}
+
 int prepare_step_kernels() {
     // Kernel attributes and occupancy are set up once, outside any stream
     // capture.
     return (blocks_per_sm<0>() > 0 && blocks_per_sm<1>() > 0 && blocks_per_sm<2>() > 0 &&
             batch_blocks_per_sm<-1>() > 0 && batch_blocks_per_sm<0>() > 0 && batch_blocks_per_sm<1>() > 0 &&
-            batch_blocks_per_sm<2>() > 0)
+            batch_blocks_per_sm<2>() > 0 && pass_blocks_per_sm_t<0>() >= 0 && pass_blocks_per_sm_t<1>() >= 0 &&
+            pass_blocks_per_sm_t<2>() >= 0)
                ? (int)cudaGetLastError()
                : 1;
+}
+
+int pass_blocks_per_sm(int mode) {
+    if (mode == 0) return pass_blocks_per_sm_t<0>();
+    if (mode == 1) return pass_blocks_per_sm_t<1>();
+    return pass_blocks_per_sm_t<2>();
+}
+
+int launch_pass(int mode, const PassParams& pp, int grid, void* stream) {
+    if (grid <= 0 || pp.nsteps <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mode == 0) return launch_pass_t<0>(pp, grid, st);
+    if (mode == 1) return launch_pass_t<1>(pp, grid, st);
+    return launch_pass_t<2>(pp, grid, st);
+}
+
+void tile_rect(const StepArgs& a, int b, int* z0, int* z1, int* x0, int* x1) {
+    int r = 0;
+    while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
+    const int t = b - a.r_first[r], type = a.r_type[r];
+    const int tzsz = (type == 0 || type == 1) ? TZ : (type == 4 ? 4 : PTZ);
+    const int txsz = type == 0 ? a.itx : (type == 4 ? RTX : (type == 2 ? ZTX : PTX));
+    const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
+    *z0 = a.r_zd0[r] + tz * tzsz;
+    *x0 = a.r_x0[r] + tx * txsz;
+    *z1 = min(*z0 + tzsz, a.r_zd0[r] + a.r_h[r]);
+    *x1 = min(*x0 + txsz, a.r_x0[r] + a.r_w[r]);
 }
 
 int launch_step(int mode, const StepArgs& a, void* stream) {

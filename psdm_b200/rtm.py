@@ -219,6 +219,10 @@ class Engine:
         """psdm_freq_filter_device: filters device traces (num, nt) in place (asynchronous)."""
         L.check(L.lib().psdm_freq_filter_device(self._h, d_traces, nt, dt, num, typef, f1, f2))
 
+    def set_pass_launch(self, on: bool):
+        """psdm_engine_set_pass_launch: one cooperative launch per pass (True) or one launch per step."""
+        L.check(L.lib().psdm_engine_set_pass_launch(self._h, int(bool(on))))
+
     def set_checkpointing(self, interval: int):
         """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
         L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))
