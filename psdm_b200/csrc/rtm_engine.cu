@@ -511,7 +511,7 @@ int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args
     int* d_flags = nullptr;
     TRY(e->get(("pass_base" + m).c_str(), 2, &d_base));
     TRY(e->get(("pass_var" + m).c_str(), var.size(), &d_var));
-    TRY(e->get("pass_flags", (size_t)ntiles, &d_flags));
+    TRY(e->get("pass_flags", (size_t)ntiles + 1, &d_flags));  // + the abort word
     // Staged through page-locked buffers, one per pass kind, refilled only
     // after the previous copy out of them has completed.
     const size_t sbytes = 2 * sizeof(StepArgs) + var.size() * sizeof(PassVar);
@@ -527,7 +527,7 @@ int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args
     CUDA_TRY(cudaMemcpyAsync(d_var, h + 2 * sizeof(StepArgs), var.size() * sizeof(PassVar), cudaMemcpyHostToDevice,
                              e->stream));
     CUDA_TRY(cudaEventRecord(done, e->stream));
-    CUDA_TRY(cudaMemsetAsync(d_flags, 0, (size_t)ntiles * sizeof(int), e->stream));
+    CUDA_TRY(cudaMemsetAsync(d_flags, 0, ((size_t)ntiles + 1) * sizeof(int), e->stream));
     PassParams pp{};
     pp.base = d_base;
     pp.var = d_var;
@@ -538,6 +538,7 @@ int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args
     pp.rec_first = d_rf;
     pp.rec_idx = d_ri;
     pp.flags = d_flags;
+    pp.abort = d_flags + ntiles;
     pp.err = a.err;
     const int rc = launch_pass(mode, pp, grid, e->stream);
     if (rc) return fail(PSDM_ERR_CUDA, "pass launch: %s", cudaGetErrorString((cudaError_t)rc));

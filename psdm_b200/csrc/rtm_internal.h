@@ -193,7 +193,8 @@ struct PassParams {
     const int* rec_first;  // [ntiles + 1]
     const int* rec_idx;    // receivers whose cell lies in each tile
     int* flags;            // [ntiles] steps completed, zero at launch
-    int* err;
+    int* abort;            // device word, zero at launch: set when a block gives up
+    int* err;              // the engine's error word (host memory mapped into the device)
 };
 
 // Cell rectangle [z0, z1) x [x0, x1) (device rows, columns) of tile b of a plan.

@@ -966,7 +966,11 @@ __device__ __forceinline__ int ld_relaxed(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 // Later bulk copies (async proxy) of this thread see what its generic-proxy
 // acquire made visible.
 __device__ __forceinline__ void fence_proxy_async_global() {
@@ -978,19 +982,18 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Wait until *flag >= need: relaxed polls, then one acquire fence.  Gives up
-// after ~1 s, or at once when another block has reported an error.
-__device__ bool wait_flag(const int* flag, int need, const int* err) {
+// Wait until *flag >= need: relaxed polls, then one acquire load.  Gives up
+// after ~1 s, or at once when another block has given up (abort, a device
+// word: polling the host-mapped error word would cost a PCIe round trip).
+__device__ bool wait_flag(const int* flag, int need, const int* abort) {
     if (ld_relaxed(flag) < need) {
         const uint64_t t0 = globaltimer_ns();
         for (int it = 0;; ++it) {
             if (ld_relaxed(flag) >= need) break;
-            if (it >= 32) __nanosleep(64);
-            if ((it & 15) == 15 && (ld_relaxed(err) != 0 || globaltimer_ns() - t0 > 1000000000ull)) return false;
+            if ((it & 15) == 15 && (ld_relaxed(abort) != 0 || globaltimer_ns() - t0 > 1000000000ull)) return false;
         }
     }
-    fence_acq_rel_gpu();
-    return true;
+    return ld_acquire(flag) >= need;  // the flag only grows
 }
 
 // All steps of one pass.  Block b owns tiles b, b + gridDim.x, ...; before
@@ -1050,27 +1053,26 @@ __global__ void __launch_bounds__(NT, 5) pass_kernel(const PassParams pp) {
         for (int T = blockIdx.x; T < pp.ntiles; T += gridDim.x) {
             bool ok = true;
             for (int k = pp.nbr_first[T] + tid; k < pp.nbr_first[T + 1]; k += NT)
-                ok = wait_flag(pp.flags + pp.nbr[k], i, pp.err) && ok;
+                ok = wait_flag(pp.flags + pp.nbr[k], i, pp.abort) && ok;
             if (__syncthreads_or(!ok)) {
                 if (tid == 0) {
+                    atomicExch(pp.abort, 1);
                     atomicCAS(pp.err, 0, 3);
                     cp_async_wait_all();
                 }
                 return;
             }
-            fence_proxy_async_global();
+            if (threadIdx.y == 0) fence_proxy_async_global();  // warp 0 issues the tile's bulk copies
             if (!run_tile<MODE, XS_ONE>(a, sm, &bar, phase, T)) {
                 if (tid == 0) {
+                    atomicExch(pp.abort, 1);
                     atomicCAS(pp.err, 0, 1);
                     cp_async_wait_all();
                 }
                 return;
             }
             __syncthreads();  // the tile's writes precede the publication; shared tile reused
-            if (tid == 0) {
-                __threadfence();
-                st_release(pp.flags + T, i + 1);
-            }
+            if (tid == 0) st_release(pp.flags + T, i + 1);  // cumulative over the block's writes
         }
     }
 }
