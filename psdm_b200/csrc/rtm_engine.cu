@@ -427,43 +427,6 @@ bool pass_form(const std::vector<StepArgs>& args, StepArgs base[2], std::vector<
            std::memcmp(b0.r_first, b1.r_first, sizeof b0.r_first) == 0;
 }
 
-// Neighbour lists of a plan (tiles within kTileReadHalo cells of each other,
-// the reach of every tile's reads) and the receivers held by each tile, both
-// as offset arrays.
-void pass_lists(const StepArgs& a, int nrec, const int* h_rec_cell, std::vector<int>* nbr_first,
-                std::vector<int>* nbr, std::vector<int>* rec_first, std::vector<int>* rec_idx) {
-    const int n = a.r_first[a.nrect];
-    std::vector<std::array<int, 4>> R(n);
-    for (int b = 0; b < n; ++b) tile_rect(a, b, &R[b][0], &R[b][1], &R[b][2], &R[b][3]);
-    const int H = kTileReadHalo;
-    nbr_first->assign(n + 1, 0);
-    nbr->clear();
-    for (int b = 0; b < n; ++b) {
-        for (int c = 0; c < n; ++c)
-            if (c != b && R[c][0] < R[b][1] + H && R[b][0] - H < R[c][1] && R[c][2] < R[b][3] + H &&
-                R[b][2] - H < R[c][3])
-                nbr->push_back(c);
-        (*nbr_first)[b + 1] = (int)nbr->size();
-    }
-    // A cell in no tile is never updated: its p stays 0, as the zeroed traces
-    // already hold.
-    std::vector<std::vector<int>> by(n);
-    for (int i = 0; i < nrec; ++i) {
-        const int x = h_rec_cell[i] / a.ldz, zd = h_rec_cell[i] % a.ldz;
-        for (int b = 0; b < n; ++b)
-            if (zd >= R[b][0] && zd < R[b][1] && x >= R[b][2] && x < R[b][3]) {
-                by[b].push_back(i);
-                break;
-            }
-    }
-    rec_first->assign(n + 1, 0);
-    rec_idx->clear();
-    for (int b = 0; b < n; ++b) {
-        rec_idx->insert(rec_idx->end(), by[b].begin(), by[b].end());
-        (*rec_first)[b + 1] = (int)rec_idx->size();
-    }
-}
-
 // One cooperative launch for the whole pass.  Returns PSDM_OK when launched,
 // 1 when the pass does not have the form (the caller launches per step), or
 // an error code.

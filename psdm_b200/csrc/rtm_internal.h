@@ -5,6 +5,7 @@
 #include <complex>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace psdm {
 
@@ -201,6 +202,11 @@ struct PassParams {
 void tile_rect(const StepArgs& a, int b, int* z0, int* z1, int* x0, int* x1);
 // Halo (cells) within which a tile's reads of p, phi and the snapshot lie.
 constexpr int kTileReadHalo = 12;
+// Neighbour lists of a plan (tiles within kTileReadHalo cells of each other)
+// and the receivers (linear cells x * ldz + row) held by each tile, both as
+// offset arrays.
+void pass_lists(const StepArgs& a, int nrec, const int* h_rec_cell, std::vector<int>* nbr_first,
+                std::vector<int>* nbr, std::vector<int>* rec_first, std::vector<int>* rec_idx);
 // Resident blocks per multiprocessor of the pass kernel (0 on failure).
 int pass_blocks_per_sm(int mode);
 // Launch one pass (modes 0, 1, 2) with `grid` co-resident blocks.

@@ -43,6 +43,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <vector>
 
@@ -1289,6 +1290,43 @@ void tile_rect(const StepArgs& a, int b, int* z0, int* z1, int* x0, int* x1) {
     *x0 = a.r_x0[r] + tx * txsz;
     *z1 = min(*z0 + tzsz, a.r_zd0[r] + a.r_h[r]);
     *x1 = min(*x0 + txsz, a.r_x0[r] + a.r_w[r]);
+}
+
+// Neighbour lists of a plan (tiles within kTileReadHalo cells of each other,
+// the reach of every tile's reads) and the receivers held by each tile, both
+// as offset arrays.
+void pass_lists(const StepArgs& a, int nrec, const int* h_rec_cell, std::vector<int>* nbr_first,
+                std::vector<int>* nbr, std::vector<int>* rec_first, std::vector<int>* rec_idx) {
+    const int n = a.r_first[a.nrect];
+    std::vector<std::array<int, 4>> R(n);
+    for (int b = 0; b < n; ++b) tile_rect(a, b, &R[b][0], &R[b][1], &R[b][2], &R[b][3]);
+    const int H = kTileReadHalo;
+    nbr_first->assign(n + 1, 0);
+    nbr->clear();
+    for (int b = 0; b < n; ++b) {
+        for (int c = 0; c < n; ++c)
+            if (c != b && R[c][0] < R[b][1] + H && R[b][0] - H < R[c][1] && R[c][2] < R[b][3] + H &&
+                R[b][2] - H < R[c][3])
+                nbr->push_back(c);
+        (*nbr_first)[b + 1] = (int)nbr->size();
+    }
+    // A cell in no tile is never updated: its p stays 0, as the zeroed traces
+    // already hold.
+    std::vector<std::vector<int>> by(n);
+    for (int i = 0; i < nrec; ++i) {
+        const int x = h_rec_cell[i] / a.ldz, zd = h_rec_cell[i] % a.ldz;
+        for (int b = 0; b < n; ++b)
+            if (zd >= R[b][0] && zd < R[b][1] && x >= R[b][2] && x < R[b][3]) {
+                by[b].push_back(i);
+                break;
+            }
+    }
+    rec_first->assign(n + 1, 0);
+    rec_idx->clear();
+    for (int b = 0; b < n; ++b) {
+        rec_idx->insert(rec_idx->end(), by[b].begin(), by[b].end());
+        (*rec_first)[b + 1] = (int)rec_idx->size();
+    }
 }
 
 int launch_step(int mode, const StepArgs& a, void* stream) {
