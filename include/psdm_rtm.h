@@ -367,6 +367,46 @@ int psdm_su_read_shot(const char* path, int32_t NumRec, int32_t ns_max, int32_t 
 int psdm_su_read_header_i32(const char* path, int32_t NumRec, int32_t ns_max, int32_t byte_pos,
                             int32_t big_endian, int32_t* out);
 
+/* ---- Survey geometry (host) ------------------------------------------------ */
+/*
+ * read_nav_shot_mcs (src/get_mcs_data.f90:30-126): the shot navigation file,
+ * one record per shot, list-directed: "shotID x" (cols 11), "shotID x y"
+ * (111) or "shotID x y depth" (1111).  pos_shot = d_shot_model + distance
+ * from the line's origin (the first shot for dir_boat = 1, the last for -1),
+ * pos_bat = |depth|.  shot_i / shot_f = 0 select the first / last record's
+ * shot; out = {nlines, line_i, line_f} (1-based records of shot_i, shot_f;
+ * the last record with the number wins).  out[0] is set even when max_lines
+ * is too small (then PSDM_ERR_ARG); a shot number not found is PSDM_ERR_ARG.
+ */
+int psdm_nav_read(const char* path, int32_t cols, int32_t dir_boat, float d_shot_model, int32_t shot_i,
+                  int32_t shot_f, int32_t max_lines, int32_t* shotID, float* pos_shot, float* pos_bat,
+                  int32_t* out /* 3 */);
+/*
+ * get_pos_channels (src/get_mcs_data.f90:418-510): channel positions of one
+ * shot, pos_rec = pos_shot - dir_boat * offset, the offset from the trace
+ * headers (offset_header = 1: |offset| * offset_unit, or |offset| /
+ * |offset_unit| when offset_unit < 0; read them with
+ * psdm_su_read_header_i32) or from the spread (offset_header = 0:
+ * near_offset + (i-1) drec).
+ */
+int psdm_channel_positions(float pos_shot, int32_t NumRec, int32_t dir_boat, int32_t offset_header,
+                           float offset_unit, const int32_t* offsets, float near_offset, float drec,
+                           float* pos_rec);
+/* get_geometry_mcs (src/get_mcs_data.f90:128-148): 1-based grid indices
+ * 1 + floor(position / dd) of the source and the channels. */
+int psdm_geometry_mcs(float pos_shot, int32_t NumRec, const float* pos_rec, float shot_depth,
+                      float streamer_depth, float dd, int32_t* nxSou, int32_t* nySou, int32_t* nxRec,
+                      int32_t* nyRec);
+/* linear_2D (src/linear_interpolation.f90:1-45, with linear_interpolation_1D
+ * :79-117): the model vel (nymodel, nxmodel) at dmodel resampled to Vpmodel
+ * (ny_prop, nx_prop) at dmodel_prop, along depth then along x. */
+int psdm_linear_2d(int32_t nxmodel, int32_t nymodel, float dmodel, const float* vel, int32_t nx_prop,
+                   int32_t ny_prop, float dmodel_prop, float* Vpmodel);
+/* Sea-floor depth per column (src/00-main.f90:146-158): (j-2) dmodel_prop for
+ * the first 1-based row j whose velocity exceeds water_velocity, else 0. */
+int psdm_batmodel_from_velocity(int32_t nx_prop, int32_t ny_prop, float dmodel_prop, float water_velocity,
+                                const float* Vpmodel, float* Batmodel);
+
 /* normalize_psdm (src/auxiliar_PSDM.f90:1-20): PSDM = sum/fold where fold > 0. */
 void psdm_normalize_psdm(int32_t nx, int32_t ny, const float* PSDM_sum, const float* Cov_sum,
                          float* PSDM);

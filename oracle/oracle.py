@@ -300,6 +300,103 @@ def freq_filter(Data_trace, dt: float, typef: int, f1: float, f2: float) -> np.n
     return D
 
 
+def nav_read(text: str, cols: int, dir_boat: int, d_shot_model: float, shot_i: int = 0, shot_f: int = 0):
+    """read_nav_shot_mcs (get_mcs_data.f90:30-126) on the file's text, in
+    single precision: (shotID, pos_shot, pos_bat, line_i, line_f), line_i /
+    line_f = 0 when the shot number is not found."""
+    f32 = np.float32
+    recs = text.split("\n")
+    if recs and recs[-1] == "":
+        recs = recs[:-1]
+    nval = {11: 2, 111: 3, 1111: 4}[cols]
+    ids, xs, ys, bat = [], [], [], []
+    for r in recs:
+        v = r.split("/")[0].replace(",", " ").split()[:nval]
+        v = [w.replace("d", "e").replace("D", "e") for w in v]
+        ids.append(int(v[0]))
+        xs.append(f32(float(v[1])))
+        ys.append(f32(float(v[2])) if nval >= 3 else f32(0))
+        bat.append(f32(float(v[3])) if nval >= 4 else f32(0))
+    n = len(ids)
+    o = 0 if dir_boat == 1 else n - 1   # get_mcs_data.f90:68-78
+    x1, y1 = xs[o], ys[o]
+    si = shot_i or ids[0]
+    sf = shot_f or ids[-1]
+    line_i = max([k + 1 for k in range(n) if ids[k] == si], default=0)
+    line_f = max([k + 1 for k in range(n) if ids[k] == sf], default=0)
+    pos = np.array([f32(d_shot_model) + np.sqrt(f32(xs[k] - x1) * f32(xs[k] - x1) + f32(ys[k] - y1) * f32(ys[k] - y1))
+                    for k in range(n)], np.float32)
+    return np.array(ids, np.int32), pos, np.abs(np.array(bat, np.float32)), line_i, line_f
+
+
+def channel_positions(pos_shot, nrec, dir_boat, offset_header, offset_unit=1.0, offsets=None, near_offset=0.0,
+                      drec=0.0) -> np.ndarray:
+    """get_pos_channels (get_mcs_data.f90:418-510) in single precision."""
+    f32 = np.float32
+    dirf = f32(dir_boat)
+    out = np.zeros(nrec, np.float32)
+    for i in range(nrec):
+        if offset_header == 1:
+            a = f32(abs(int(offsets[i])))
+            off = a * f32(offset_unit) if offset_unit > 0 else a / f32(abs(offset_unit))
+        else:
+            off = f32(near_offset) + f32(i) * f32(drec)
+        out[i] = f32(pos_shot) - dirf * f32(off)
+    return out
+
+
+def geometry_mcs(pos_shot, pos_rec, shot_depth, streamer_depth, dd):
+    """get_geometry_mcs (get_mcs_data.f90:128-148): 1 + floor(position / dd)."""
+    f32 = np.float32
+    g = lambda v: 1 + int(np.floor(f32(v) / f32(dd)))
+    return (g(pos_shot), g(shot_depth), np.array([g(v) for v in pos_rec], np.int32),
+            np.full(len(pos_rec), g(streamer_depth), np.int32))
+
+
+def _linear_1d(x1, y1, x2):
+    """linear_interpolation_1D (linear_interpolation.f90:79-117) in single precision."""
+    y2 = np.zeros(len(x2), np.float32)
+    n1 = len(x1)
+    for j, a3 in enumerate(x2):
+        if a3 <= x1[0]:
+            y2[j] = y1[0]
+        elif a3 >= x1[n1 - 1]:
+            y2[j] = y1[n1 - 1]
+        else:
+            for i in range(n1 - 1):
+                a1, a2, b1, b2 = x1[i + 1], x1[i], y1[i + 1], y1[i]
+                if a2 <= a3 <= a1 and abs(b1) > 0 and abs(b2) > 0:
+                    m = np.float32(b1 - b2) / np.float32(a1 - a2)
+                    y2[j] = np.float32(b2 + np.float32(np.float32(a3 - a2) * m))
+                    break
+    return y2
+
+
+def linear_2d(vel, dmodel, nx_prop, ny_prop, dmodel_prop) -> np.ndarray:
+    """linear_2D (linear_interpolation.f90:1-45): vel (nxmodel, nymodel) to (nx_prop, ny_prop)."""
+    f32 = np.float32
+    vel = np.asarray(vel, np.float32)
+    nxm, nym = vel.shape
+    xm = np.array([f32(i) * f32(dmodel) for i in range(nxm)], np.float32)
+    ym = np.array([f32(i) * f32(dmodel) for i in range(nym)], np.float32)
+    xp = np.array([f32(i) * f32(dmodel_prop) for i in range(nx_prop)], np.float32)
+    yp = np.array([f32(i) * f32(dmodel_prop) for i in range(ny_prop)], np.float32)
+    tmp = np.stack([_linear_1d(ym, vel[i], yp) for i in range(nxm)])           # (nxm, ny_prop)
+    out = np.stack([_linear_1d(xm, tmp[:, j], xp) for j in range(ny_prop)], 1)  # (nx_prop, ny_prop)
+    return out.astype(np.float32)
+
+
+def batmodel_from_velocity(Vpmodel, dmodel_prop, water_velocity) -> np.ndarray:
+    """00-main.f90:146-158: (j-2) dmodel_prop at the first 1-based row j with V > water_velocity."""
+    v = np.asarray(Vpmodel, np.float32)
+    out = np.zeros(v.shape[0], np.float32)
+    for i in range(v.shape[0]):
+        j = np.flatnonzero(v[i] > np.float32(water_velocity))
+        if j.size:
+            out[i] = np.float32(j[0] - 1) * np.float32(dmodel_prop)
+    return out
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a = _f32(psdm_sum)
     b = _f32(cov_sum)

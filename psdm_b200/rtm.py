@@ -328,6 +328,63 @@ def su_read_header_i32(path: str, nrec: int, ns_max: int, byte_pos: int, big_end
     return out
 
 
+def nav_read(path: str, cols: int, dir_boat: int, d_shot_model: float, shot_i: int = 0, shot_f: int = 0):
+    """psdm_nav_read: (shotID, pos_shot, pos_bat, line_i, line_f) of a shot navigation file."""
+    out = np.zeros(3, np.int32)
+    L.lib().psdm_nav_read(str(path).encode(), cols, dir_boat, d_shot_model, shot_i, shot_f, 0, None, None, None,
+                          out)
+    n = int(out[0])
+    if n <= 0:
+        L.check(L.lib().psdm_nav_read(str(path).encode(), cols, dir_boat, d_shot_model, shot_i, shot_f, 0, None,
+                                      None, None, out))
+    ids = np.zeros(n, np.int32)
+    pos = np.zeros(n, np.float32)
+    bat = np.zeros(n, np.float32)
+    L.check(L.lib().psdm_nav_read(str(path).encode(), cols, dir_boat, d_shot_model, shot_i, shot_f, n,
+                                  ids.ctypes.data, pos.ctypes.data, bat.ctypes.data, out))
+    return ids, pos, bat, int(out[1]), int(out[2])
+
+
+def channel_positions(pos_shot: float, nrec: int, dir_boat: int, offset_header: int, offset_unit: float = 1.0,
+                      offsets=None, near_offset: float = 0.0, drec: float = 0.0):
+    """psdm_channel_positions: pos_rec (nrec,) of one shot."""
+    out = np.zeros(nrec, np.float32)
+    off = None if offsets is None else _i32(offsets)
+    L.check(L.lib().psdm_channel_positions(pos_shot, nrec, dir_boat, offset_header, offset_unit,
+                                           None if off is None else off.ctypes.data, near_offset, drec, out))
+    return out
+
+
+def geometry_mcs(pos_shot: float, pos_rec, shot_depth: float, streamer_depth: float, dd: float):
+    """psdm_geometry_mcs: (nxSou, nySou, nxRec, nyRec), 1-based grid indices."""
+    pr = _f32(pos_rec).reshape(-1)
+    nxs, nys = C.c_int32(), C.c_int32()
+    nxr = np.zeros(pr.size, np.int32)
+    nyr = np.zeros(pr.size, np.int32)
+    L.check(L.lib().psdm_geometry_mcs(pos_shot, pr.size, pr, shot_depth, streamer_depth, dd, C.byref(nxs),
+                                      C.byref(nys), nxr, nyr))
+    return nxs.value, nys.value, nxr, nyr
+
+
+def linear_2d(vel, dmodel: float, nx_prop: int, ny_prop: int, dmodel_prop: float) -> np.ndarray:
+    """psdm_linear_2d: vel (nxmodel, nymodel) resampled to (nx_prop, ny_prop)."""
+    v = _f32(vel)
+    nxm, nym = v.shape
+    out = np.zeros((nx_prop, ny_prop), np.float32)
+    L.check(L.lib().psdm_linear_2d(nxm, nym, dmodel, v.reshape(-1), nx_prop, ny_prop, dmodel_prop,
+                                   out.reshape(-1)))
+    return out
+
+
+def batmodel_from_velocity(Vpmodel, dmodel_prop: float, water_velocity: float) -> np.ndarray:
+    """psdm_batmodel_from_velocity: sea-floor depth (nx_prop,) from Vpmodel (nx_prop, ny_prop)."""
+    v = _f32(Vpmodel)
+    nx, ny = v.shape
+    out = np.zeros(nx, np.float32)
+    L.check(L.lib().psdm_batmodel_from_velocity(nx, ny, dmodel_prop, water_velocity, v.reshape(-1), out))
+    return out
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a, b = _f32(psdm_sum), _f32(cov_sum)
     out = np.zeros_like(a)
