@@ -407,6 +407,40 @@ int psdm_linear_2d(int32_t nxmodel, int32_t nymodel, float dmodel, const float* 
 int psdm_batmodel_from_velocity(int32_t nx_prop, int32_t ny_prop, float dmodel_prop, float water_velocity,
                                 const float* Vpmodel, float* Batmodel);
 
+/*
+ * Wide-angle (OBS) data: by reciprocity the OBSs are the sources and the shots
+ * the receivers.  read_nav_shot_was (src/get_was_data.f90:70-125): the first
+ * NumShots records "shotID x [y [depth]]" (cols 11 / 111 / 1111);
+ * pos_shot = d_shot_model + distance from the first shot, pos_bat = |depth|;
+ * out_i = {line_i, line_f (0 when the number is absent), nxmodel_was =
+ * 1 + ceiling(length_model_was / dmodel)}, out_f = {dshots_was,
+ * length_model_was = last shot's x + 2 added_space}.
+ */
+int psdm_nav_read_was(const char* path, int32_t cols, int32_t NumShots, float d_shot_model, float added_space,
+                      float dmodel, int32_t shot_i, int32_t shot_f, int32_t* shotID, float* pos_shot,
+                      float* pos_bat, int32_t* out_i /* 3 */, float* out_f /* 2 */);
+/* read_nav_obs (src/get_was_data.f90:127-160): NumOBS records "obsID x z";
+ * positions |x|, |z| and their grid indices 1 + ceiling(position / dmodel). */
+int psdm_nav_read_obs(const char* path, int32_t NumOBS, float dmodel, int32_t* obsID, float* pos_xobs,
+                      float* pos_zobs, int32_t* xgrid, int32_t* zgrid);
+/* get_geometry_WAS (src/get_was_data.f90:162-189): the OBS's grid indices as
+ * the source, 1 + ceiling(position / dd) of the shots as the receivers. */
+int psdm_geometry_was(int32_t xobs_grid, int32_t zobs_grid, int32_t NumRec, const float* pos_shot,
+                      float shot_depth, float dd, int32_t* nxSou, int32_t* nySou, int32_t* nxRec,
+                      int32_t* nyRec);
+/* get_bathymetry_model_was / _mcs (src/get_was_data.f90:500-549,
+ * src/get_mcs_data.f90:353-415): sea-floor depth at x = (i-1) dmodel along
+ * the line, Akima's interpolant through (0, first depth), the shots
+ * (pos_shot, pos_bat) and (length_model, last depth).  Positions must
+ * increase strictly. */
+int psdm_bathymetry_nav(int32_t NumShots, const float* pos_shot, const float* pos_bat, float length_model,
+                        int32_t nxmodel, float dmodel, float* bat_model);
+/* relocation_zOBS (src/get_was_data.f90:30-68): each OBS moved to the sea
+ * floor under it, pos_zobs = bat_model(xgrid), zgrid = 1 + ceiling(pos_zobs /
+ * dmodel). */
+int psdm_relocate_obs(int32_t NumOBS, const int32_t* xgrid, const float* bat_model, int32_t nxmodel,
+                      float dmodel, float* pos_zobs, int32_t* zgrid);
+
 /* normalize_psdm (src/auxiliar_PSDM.f90:1-20): PSDM = sum/fold where fold > 0. */
 void psdm_normalize_psdm(int32_t nx, int32_t ny, const float* PSDM_sum, const float* Cov_sum,
                          float* PSDM);

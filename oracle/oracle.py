@@ -397,6 +397,118 @@ def batmodel_from_velocity(Vpmodel, dmodel_prop, water_velocity) -> np.ndarray:
     return out
 
 
+def _records(text: str, nrec: int, nval: int):
+    recs = text.split("\n")
+    out = []
+    for r in recs[:nrec]:
+        v = r.split("/")[0].replace(",", " ").split()[:nval]
+        v = [w.replace("d", "e").replace("D", "e") for w in v]
+        out.append([int(v[0])] + [np.float32(float(w)) for w in v[1:]])
+    return out
+
+
+def nav_read_was(text: str, cols: int, num_shots: int, d_shot_model, added_space, dmodel, shot_i=0, shot_f=0):
+    """read_nav_shot_was (get_was_data.f90:70-125) in single precision."""
+    f32 = np.float32
+    nval = {11: 2, 111: 3, 1111: 4}[cols]
+    rec = _records(text, num_shots, nval)
+    xs = [r[1] for r in rec]
+    ys = [r[2] if nval >= 3 else f32(0) for r in rec]
+    bat = [r[3] if nval >= 4 else f32(0) for r in rec]
+    x1, y1 = xs[0], ys[0]
+    ids = np.array([r[0] for r in rec], np.int32)
+    pos = np.array([f32(d_shot_model) + np.sqrt(f32(xs[k] - x1) * f32(xs[k] - x1) + f32(ys[k] - y1) * f32(ys[k] - y1))
+                    for k in range(num_shots)], np.float32)
+    li = max([k + 1 for k in range(num_shots) if ids[k] == shot_i], default=0)
+    lf = max([k + 1 for k in range(num_shots) if ids[k] == shot_f], default=0)
+    xn = xs[-1]
+    length = f32(xn + f32(f32(2) * f32(added_space)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        dsh = f32(abs(f32(xn - x1)) / f32(num_shots - 1))
+    nxm = 1 + int(np.ceil(f32(length / f32(dmodel))))
+    return ids, pos, np.abs(np.array(bat, np.float32)), (li, lf, nxm), (float(dsh), float(length))
+
+
+def nav_read_obs(text: str, num_obs: int, dmodel):
+    """read_nav_obs (get_was_data.f90:127-160) in single precision."""
+    f32 = np.float32
+    rec = _records(text, num_obs, 3)
+    px = np.abs(np.array([r[1] for r in rec], np.float32))
+    pz = np.abs(np.array([r[2] for r in rec], np.float32))
+    g = lambda v: np.array([1 + int(np.ceil(f32(x / f32(dmodel)))) for x in v], np.int32)
+    return np.array([r[0] for r in rec], np.int32), px, pz, g(px), g(pz)
+
+
+def geometry_was(xobs_grid, zobs_grid, pos_shot, shot_depth, dd):
+    """get_geometry_WAS (get_was_data.f90:162-189): 1 + ceiling(position / dd) for the shots."""
+    f32 = np.float32
+    g = lambda v: 1 + int(np.ceil(f32(v) / f32(dd)))
+    return (xobs_grid, zobs_grid, np.array([g(v) for v in pos_shot], np.int32),
+            np.full(len(pos_shot), g(shot_depth), np.int32))
+
+
+def akima_nonuniform(x, y, u):
+    """Akima's interpolant (J. ACM 17 (1970) 589-602) through (x, y), x
+    strictly increasing, at the points u; single precision, in the order the
+    engine evaluates it (slopes extended by two per side, node-slope weights
+    |m_{i+1}-m_i| and |m_{i-1}-m_{i-2}|, end intervals continued outside)."""
+    f32 = np.float32
+    x = [f32(v) for v in x]
+    y = [f32(v) for v in y]
+    n = len(x)
+    M = [f32(0)] * (n + 3)
+    for i in range(n - 1):
+        M[i + 2] = f32(f32(y[i + 1] - y[i]) / f32(x[i + 1] - x[i]))
+    if n == 2:
+        M[0] = M[1] = M[3] = M[4] = M[2]
+    else:
+        M[1] = f32(f32(2) * M[2] - M[3])
+        M[0] = f32(f32(2) * M[1] - M[2])
+        M[n + 1] = f32(f32(2) * M[n] - M[n - 1])
+        M[n + 2] = f32(f32(2) * M[n + 1] - M[n])
+    t = []
+    for i in range(n):
+        w1 = f32(abs(f32(M[i + 3] - M[i + 2])))
+        w2 = f32(abs(f32(M[i + 1] - M[i])))
+        w = f32(w1 + w2)
+        t.append(f32(f32(M[i + 1] + M[i + 2]) * f32(0.5)) if w == 0 else
+                 f32(f32(f32(w1 * M[i + 1]) + f32(w2 * M[i + 2])) / w))
+    out = np.zeros(len(u), np.float32)
+    for k, uu in enumerate(u):
+        uu = f32(uu)
+        if uu == x[-1]:
+            out[k] = y[-1]
+            continue
+        if uu >= x[-1]:
+            i = n - 2
+        elif uu > x[0]:
+            i = max(j for j in range(n - 1) if x[j] <= uu)
+        else:
+            i = 0
+        h = f32(x[i + 1] - x[i])
+        d = f32(uu - x[i])
+        m, t0, t1 = M[i + 2], t[i], t[i + 1]
+        c2 = f32(f32(f32(f32(f32(3) * m) - f32(f32(2) * t0)) - t1) / h)
+        c3 = f32(f32(f32(t0 + t1) - f32(f32(2) * m)) / f32(h * h))
+        out[k] = f32(y[i] + f32(d * f32(t0 + f32(d * f32(c2 + f32(d * c3))))))
+    return out
+
+
+def bathymetry_nav(pos_shot, pos_bat, length_model, nxmodel, dmodel) -> np.ndarray:
+    """get_bathymetry_model_was / _mcs: Akima through (0, first), the shots, (length_model, last)."""
+    f32 = np.float32
+    x = [f32(0)] + [f32(v) for v in pos_shot] + [f32(length_model)]
+    y = [f32(pos_bat[0])] + [f32(v) for v in pos_bat] + [f32(pos_bat[-1])]
+    return akima_nonuniform(x, y, [f32(f32(i) * f32(dmodel)) for i in range(nxmodel)])
+
+
+def relocate_obs(xgrid, bat_model, dmodel):
+    """relocation_zOBS (get_was_data.f90:30-68)."""
+    f32 = np.float32
+    pz = np.array([bat_model[g - 1] for g in xgrid], np.float32)
+    return pz, np.array([1 + int(np.ceil(f32(v / f32(dmodel)))) for v in pz], np.int32)
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a = _f32(psdm_sum)
     b = _f32(cov_sum)

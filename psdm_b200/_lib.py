@@ -27,6 +27,7 @@ EXPORTS = [
     "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch",
     "psdm_freq_filter", "psdm_freq_filter_device",
     "psdm_nav_read", "psdm_channel_positions", "psdm_geometry_mcs", "psdm_linear_2d", "psdm_batmodel_from_velocity",
+    "psdm_nav_read_was", "psdm_nav_read_obs", "psdm_geometry_was", "psdm_bathymetry_nav", "psdm_relocate_obs",
 ]
 
 
@@ -114,6 +115,12 @@ def lib():
                                     _i32p]
     L.psdm_linear_2d.argtypes = [_I, _I, _F, _f32p, _I, _I, _F, _f32p]
     L.psdm_batmodel_from_velocity.argtypes = [_I, _I, _F, _F, _f32p, _f32p]
+    L.psdm_nav_read_was.argtypes = [C.c_char_p, _I, _I, _F, _F, _F, _I, _I, _i32p, _f32p, _f32p, _i32p, _f32p]
+    L.psdm_nav_read_obs.argtypes = [C.c_char_p, _I, _F, _i32p, _f32p, _f32p, _i32p, _i32p]
+    L.psdm_geometry_was.argtypes = [_I, _I, _I, _f32p, _F, _F, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _i32p,
+                                    _i32p]
+    L.psdm_bathymetry_nav.argtypes = [_I, _f32p, _f32p, _F, _I, _F, _f32p]
+    L.psdm_relocate_obs.argtypes = [_I, _i32p, _f32p, _I, _F, _f32p, _i32p]
     CP = C.POINTER(Conditioning)
     L.psdm_trace_windows.argtypes = [CP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _i32p, _i32p, _i32p]
     L.psdm_trace_windows.restype = None

@@ -385,6 +385,60 @@ def batmodel_from_velocity(Vpmodel, dmodel_prop: float, water_velocity: float) -
     return out
 
 
+def nav_read_was(path: str, cols: int, num_shots: int, d_shot_model: float, added_space: float, dmodel: float,
+                 shot_i: int = 0, shot_f: int = 0):
+    """psdm_nav_read_was: (shotID, pos_shot, pos_bat, (line_i, line_f, nxmodel_was),
+    (dshots_was, length_model_was))."""
+    ids = np.zeros(num_shots, np.int32)
+    pos = np.zeros(num_shots, np.float32)
+    bat = np.zeros(num_shots, np.float32)
+    oi = np.zeros(3, np.int32)
+    of = np.zeros(2, np.float32)
+    L.check(L.lib().psdm_nav_read_was(str(path).encode(), cols, num_shots, d_shot_model, added_space, dmodel,
+                                      shot_i, shot_f, ids, pos, bat, oi, of))
+    return ids, pos, bat, tuple(int(v) for v in oi), (float(of[0]), float(of[1]))
+
+
+def nav_read_obs(path: str, num_obs: int, dmodel: float):
+    """psdm_nav_read_obs: (obsID, pos_xobs, pos_zobs, xgrid, zgrid)."""
+    ids = np.zeros(num_obs, np.int32)
+    px = np.zeros(num_obs, np.float32)
+    pz = np.zeros(num_obs, np.float32)
+    gx = np.zeros(num_obs, np.int32)
+    gz = np.zeros(num_obs, np.int32)
+    L.check(L.lib().psdm_nav_read_obs(str(path).encode(), num_obs, dmodel, ids, px, pz, gx, gz))
+    return ids, px, pz, gx, gz
+
+
+def geometry_was(xobs_grid: int, zobs_grid: int, pos_shot, shot_depth: float, dd: float):
+    """psdm_geometry_was: (nxSou, nySou, nxRec, nyRec)."""
+    ps = _f32(pos_shot).reshape(-1)
+    nxs, nys = C.c_int32(), C.c_int32()
+    nxr = np.zeros(ps.size, np.int32)
+    nyr = np.zeros(ps.size, np.int32)
+    L.check(L.lib().psdm_geometry_was(xobs_grid, zobs_grid, ps.size, ps, shot_depth, dd, C.byref(nxs), C.byref(nys),
+                                      nxr, nyr))
+    return nxs.value, nys.value, nxr, nyr
+
+
+def bathymetry_nav(pos_shot, pos_bat, length_model: float, nxmodel: int, dmodel: float) -> np.ndarray:
+    """psdm_bathymetry_nav: sea-floor depth (nxmodel,) along the line."""
+    ps, pb = _f32(pos_shot).reshape(-1), _f32(pos_bat).reshape(-1)
+    out = np.zeros(nxmodel, np.float32)
+    L.check(L.lib().psdm_bathymetry_nav(ps.size, ps, pb, length_model, nxmodel, dmodel, out))
+    return out
+
+
+def relocate_obs(xgrid, bat_model, dmodel: float):
+    """psdm_relocate_obs: (pos_zobs, zgrid) of the OBSs moved to the sea floor."""
+    gx = _i32(xgrid)
+    bm = _f32(bat_model).reshape(-1)
+    pz = np.zeros(gx.size, np.float32)
+    gz = np.zeros(gx.size, np.int32)
+    L.check(L.lib().psdm_relocate_obs(gx.size, gx, bm, bm.size, dmodel, pz, gz))
+    return pz, gz
+
+
 def normalize_psdm(psdm_sum, cov_sum) -> np.ndarray:
     a, b = _f32(psdm_sum), _f32(cov_sum)
     out = np.zeros_like(a)

@@ -131,3 +131,96 @@ def test_geometry_chain_feeds_the_windows(engine_lib, oracle, tmp_path):
     assert nxr.max() < nxs and nxr.min() >= 1
     nx_w, x_i, x_f = oracle.dynamic_window(nxs, nxr, 10.0, 1400, 500.0)
     assert 1 <= x_i <= nxr.min() and x_f >= nxs and nx_w == x_f - x_i + 1
+
+
+def _obs_text(n, seed):
+    rng = np.random.default_rng(seed)
+    xs = np.sort(rng.uniform(1000.0, 30000.0, n))
+    zs = -rng.uniform(800.0, 3000.0, n)
+    return "".join(f"{k + 1} {float(xs[k])!r} {float(zs[k])!r}\n" for k in range(n))
+
+
+@pytest.mark.parametrize("cols", [11, 111, 1111])
+def test_nav_was_matches_oracle(engine_lib, oracle, tmp_path, cols):
+    from psdm_b200 import rtm
+    text = _nav_text(40, cols, seed=20 + cols)
+    p = tmp_path / "nav_was.txt"
+    p.write_text(text + "999 1.0 2.0 3.0\n")  # records beyond NumShots are not read
+    got = rtm.nav_read_was(p, cols, 40, 250.0, 2500.0, 12.5, shot_i=1003, shot_f=1030)
+    want = oracle.nav_read_was(text, cols, 40, 250.0, 2500.0, 12.5, 1003, 1030)
+    for g, w in zip(got[:3], want[:3]):
+        _same(g, w)
+    assert got[3] == want[3] and got[3][:2] == (4, 31)
+    assert got[4] == want[4]
+    from psdm_b200._lib import PsdmError
+    with pytest.raises(PsdmError, match="expected"):
+        rtm.nav_read_was(p, cols, 60, 250.0, 2500.0, 12.5)
+
+
+def test_nav_obs_and_geometry_was_match_oracle(engine_lib, oracle, tmp_path):
+    from psdm_b200 import rtm
+    text = _obs_text(12, seed=5)
+    p = tmp_path / "nav_obs.txt"
+    p.write_text(text)
+    got = rtm.nav_read_obs(p, 12, 12.5)
+    want = oracle.nav_read_obs(text, 12, 12.5)
+    for g, w in zip(got, want):
+        _same(g, w)
+    shots = rtm.nav_read_was(_write(tmp_path, _nav_text(40, 11, seed=2)), 11, 40, 0.0, 0.0, 12.5)[1]
+    g2 = rtm.geometry_was(int(got[3][4]), int(got[4][4]), shots, 7.5, 6.25)
+    w2 = oracle.geometry_was(int(got[3][4]), int(got[4][4]), shots, 7.5, 6.25)
+    assert g2[:2] == w2[:2]
+    _same(g2[2], w2[2])
+    _same(g2[3], w2[3])
+
+
+def _write(tmp_path, text, name="n.txt"):
+    p = tmp_path / name
+    p.write_text(text)
+    return p
+
+
+@pytest.mark.parametrize("nshots", [1, 2, 5, 40])
+def test_bathymetry_nav_matches_oracle(engine_lib, oracle, nshots):
+    from psdm_b200 import rtm
+    rng = np.random.default_rng(nshots)
+    pos = np.sort(rng.uniform(100.0, 9800.0, nshots)).astype(np.float32)
+    bat = rng.uniform(800.0, 2500.0, nshots).astype(np.float32)
+    nxm = 801
+    got = rtm.bathymetry_nav(pos, bat, 10000.0, nxm, 12.5)
+    _same(got, oracle.bathymetry_nav(pos, bat, 10000.0, nxm, 12.5))
+    # the interpolant passes through the shots and holds the end depths
+    assert got[0] == bat[0] and got[-1] == bat[-1]
+
+
+def test_akima_reproduces_cubic_free_cases(oracle):
+    """Akima's method is exact for straight lines and returns its nodes."""
+    from psdm_b200 import rtm
+    x = np.array([0.0, 3.0, 4.5, 9.0, 10.0, 14.0], np.float32)
+    y = (2.0 + 0.5 * x).astype(np.float32)
+    u = np.linspace(0, 14, 57).astype(np.float32)
+    v = oracle.akima_nonuniform(x, y, u)
+    assert np.allclose(v, 2.0 + 0.5 * u, atol=1e-5)
+    assert np.array_equal(oracle.akima_nonuniform(x, y, x), y)
+    got = rtm.bathymetry_nav(x[1:-1], y[1:-1], 14.0, 15, 1.0)
+    assert np.isfinite(got).all()
+
+
+def test_bathymetry_rejects_unordered_shots(engine_lib):
+    from psdm_b200 import rtm
+    from psdm_b200._lib import PsdmError
+    with pytest.raises(PsdmError, match="increase"):
+        rtm.bathymetry_nav(np.array([5.0, 3.0], np.float32), np.ones(2, np.float32), 10.0, 11, 1.0)
+
+
+def test_relocate_obs_matches_oracle(engine_lib, oracle):
+    from psdm_b200 import rtm
+    bm = np.linspace(900.0, 2100.0, 500).astype(np.float32)
+    xg = np.array([1, 17, 250, 500], np.int32)
+    got = rtm.relocate_obs(xg, bm, 12.5)
+    want = oracle.relocate_obs(xg, bm, 12.5)
+    _same(got[0], want[0])
+    _same(got[1], want[1])
+    from psdm_b200._lib import PsdmError
+    with pytest.raises(PsdmError, match="outside"):
+        rtm.relocate_obs(np.array([501], np.int32), bm, 12.5)
