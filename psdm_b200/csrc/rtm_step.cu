@@ -24,17 +24,19 @@
 // one division, (p3-p1)*0.5/dt, uses a reciprocal with an exact FMA
 // correction that the host proves correctly rounded for the shot's dt.
 //
-// Work decomposition (one launch, two block roles, see plan_tiles):
-//  * interior tiles, 128 rows x 32 columns of the interior band: p staged in
-//    shared memory with a 4-row / 3-column halo; each thread owns 4
-//    consecutive rows (one float4) of 8 consecutive columns and slides a
-//    7-column float4 window through registers (three 16-byte shared loads
-//    per 4 cells, float4 global traffic).  The free-surface row and
-//    injection rows are handled inline.
-//  * boundary tiles, 32 rows x 16 columns over the C-PML strips and the rows
-//    outside the interior band: generic per-cell update, 4 cells a thread.
+// Work decomposition (see plan_tiles): rectangles of five tile types.
+//  * interior tiles, 128 rows x 28 columns (one shot per launch) or 32
+//    columns (batched launches) of the interior band: p staged in shared
+//    memory with a 4-row / 3-column halo by bulk copies; each thread owns 4
+//    consecutive rows (one float4) of 7 or 8 consecutive columns and slides
+//    a 7-column float4 window through registers (three 16-byte shared loads
+//    per 4 cells, float4 global traffic).
+//  * C-PML x-strip, z-strip and corner tiles, and interior rows holding
+//    injection points or the free surface (4-row bands), each with its own
+//    specialised or generic per-cell update.
 // Rows are offset by `zoff` so that the interior starts on a 16-byte
-// boundary.
+// boundary.  step_kernel runs one step of one shot, batch_step_kernel one
+// step of several shots, pass_kernel all steps of one pass (opt-in).
 //
 // Memory: p1 is overwritten in place with p3; phi is ping-ponged because its
 // strip stencil reads neighbours; chi is updated in place.
