@@ -1,5 +1,6 @@
-"""Per-shot inputs of a marine (MCS) line, read from its files the way the
-reference prepares them before migrating a shot.
+"""Per-shot inputs of a marine (MCS) line or a wide-angle (OBS) line, read
+from their files the way the reference prepares them before migrating a shot
+(wide-angle: `WasLine`, `load_was`, `was_inputs`, after get_was_data.f90).
 
 At start-up the reference reads the shot navigation (read_nav_shot_mcs,
 src/get_mcs_data.f90:30-126) and, for every shot, its channel positions and
@@ -98,3 +99,83 @@ def shot_inputs(cfg: McsLine, geom: LineGeometry, k: int, icount: int) -> dict:
     raw, delayed = rtm.su_read_shot(cfg.su_paths[icount - 1], cfg.num_rec, cfg.ns_max, cfg.nt, cfg.big_endian, d)
     return dict(shot_id=int(geom.shot_id[icount - 1]), nxSou=geom.nxSou[k], nySou=geom.nySou[k],
                 nxRec=geom.nxRec[k], nyRec=geom.nyRec[k], Field_Data=delayed if cfg.delay_time != 0 else raw)
+
+
+# ---- wide-angle (OBS) data -------------------------------------------------
+
+@dataclass
+class WasLine:
+    """Parfile values of a wide-angle line: OBS gathers, in which by
+    reciprocity the OBSs act as sources and the shots as receivers."""
+    nav_shot_path: str                 # folder_input_was // nav_shot_was
+    nav_obs_path: str                  # folder_input_was // nav_obs
+    su_paths: List[str]                # one SU gather per OBS (su_file_was)
+    num_shots: int                     # NumShots_was (= NumRec_WAS)
+    num_obs: int                       # NumOBS
+    ns_max: int                        # nt_was_max
+    nt: int                            # nt_was
+    dd: float                          # dmodel_prop
+    dmodel: float                      # dmodel: grid of the model and of the OBS indices
+    length_model: float                # length_model
+    nxmodel: int                       # nxmodel
+    cols: int = 1111                   # nav_was_cols
+    d_shot_model: float = 0.0          # d_shot_model
+    added_space: float = 0.0           # added_space
+    shot_i: int = 0
+    shot_f: int = 0
+    shot_depth: float = 0.0            # shot_depth_was
+    big_endian: bool = False
+
+
+@dataclass
+class WasGeometry:
+    shot_id: np.ndarray
+    pos_shot: np.ndarray
+    pos_bat: np.ndarray
+    lines: tuple                       # (line_i, line_f, nxmodel_was)
+    spacing: tuple                     # (dshots_was, length_model_was)
+    obs_id: np.ndarray
+    pos_xobs: np.ndarray
+    pos_zobs: np.ndarray
+    xgrid: np.ndarray
+    zgrid: np.ndarray
+    bat_model: np.ndarray
+    nxSou: List[int] = field(default_factory=list)
+    nySou: List[int] = field(default_factory=list)
+    nxRec: List[np.ndarray] = field(default_factory=list)
+    nyRec: List[np.ndarray] = field(default_factory=list)
+
+
+def load_was(cfg: WasLine) -> WasGeometry:
+    """read_nav_shot_was, read_nav_obs and get_bathymetry_model_was (the last
+    only with depths in the navigation, cols 1111; the bathymetry is zero
+    otherwise), then per OBS get_geometry_WAS followed by relocation_zOBS
+    (src/00-main.f90:62-71,195-204; get_was_data.f90:9-28).  In that order
+    the first OBS takes its source row from the navigation depth and the
+    others from the relocated one, which this reproduces."""
+    ids, pos, bat, lines, spacing = rtm.nav_read_was(cfg.nav_shot_path, cfg.cols, cfg.num_shots, cfg.d_shot_model,
+                                                     cfg.added_space, cfg.dmodel, cfg.shot_i, cfg.shot_f)
+    oid, px, pz, gx, gz = rtm.nav_read_obs(cfg.nav_obs_path, cfg.num_obs, cfg.dmodel)
+    if cfg.cols == 1111:
+        bm = rtm.bathymetry_nav(pos, bat, cfg.length_model, cfg.nxmodel, cfg.dmodel)
+    else:
+        bm = np.zeros(cfg.nxmodel, np.float32)
+    g = WasGeometry(ids, pos, bat, lines, spacing, oid, px, pz, gx, gz, bm)
+    for i in range(cfg.num_obs):
+        nxs, nys, nxr, nyr = rtm.geometry_was(int(g.xgrid[i]), int(g.zgrid[i]), pos, cfg.shot_depth, cfg.dd)
+        g.nxSou.append(nxs)
+        g.nySou.append(nys)
+        g.nxRec.append(nxr)
+        g.nyRec.append(nyr)
+        g.pos_zobs, g.zgrid = rtm.relocate_obs(g.xgrid, bm, cfg.dmodel)
+    return g
+
+
+def was_inputs(cfg: WasLine, geom: WasGeometry, iobs: int) -> dict:
+    """Field_Data (NumShots, nt) and the geometry of OBS `iobs` (1-based),
+    read as get_obs_data does (get_was_data.f90:191-227: num_shots traces, no
+    delay shift)."""
+    raw, _ = rtm.su_read_shot(cfg.su_paths[iobs - 1], cfg.num_shots, cfg.ns_max, cfg.nt, cfg.big_endian, 0)
+    k = iobs - 1
+    return dict(obs_id=int(geom.obs_id[k]), nxSou=geom.nxSou[k], nySou=geom.nySou[k], nxRec=geom.nxRec[k],
+                nyRec=geom.nyRec[k], Field_Data=raw)

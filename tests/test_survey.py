@@ -97,3 +97,47 @@ def test_spread_geometry_without_headers(engine_lib, oracle, line):
         pr = oracle.channel_positions(pos[icount - 1], NREC, -1, 0, near_offset=150.0, drec=25.0)
         assert np.array_equal(g.pos_rec[k], pr)
         assert g.nxRec[k].min() > g.nxSou[k]   # dir_boat = -1: channels at larger x
+
+
+@pytest.fixture
+def was_line(tmp_path):
+    rng = np.random.default_rng(5)
+    nshots, nobs = 40, 3
+    xs = 300000.0 + 50.0 * np.arange(nshots)
+    nav = "".join(f"{100 + k} {float(xs[k])!r} 4000000.0 {-1200.0 - 10.0 * np.sin(k / 5):.4f}\n"
+                  for k in range(nshots))
+    (tmp_path / "nav_was.txt").write_text(nav)
+    obs = "".join(f"{k + 1} {500.0 + 700.0 * k!r} {-1150.0 - 20.0 * k!r}\n" for k in range(nobs))
+    (tmp_path / "nav_obs.txt").write_text(obs)
+    paths, gathers = [], []
+    for k in range(nobs):
+        g = rng.standard_normal((nshots, NS_MAX)).astype(np.float32)
+        p = str(tmp_path / f"obs{k}.su")
+        _write_su(p, g, np.zeros(nshots, np.int32), k + 1)
+        paths.append(p)
+        gathers.append(g)
+    return tmp_path, nav, obs, paths, gathers
+
+
+def test_was_geometry_matches_oracle(engine_lib, oracle, was_line):
+    from psdm_b200 import survey
+    tmp_path, nav, obs, paths, gathers = was_line
+    cfg = survey.WasLine(nav_shot_path=str(tmp_path / "nav_was.txt"), nav_obs_path=str(tmp_path / "nav_obs.txt"),
+                         su_paths=paths, num_shots=40, num_obs=3, ns_max=NS_MAX, nt=NT, dd=12.5, dmodel=12.5,
+                         length_model=2600.0, nxmodel=209, cols=1111, d_shot_model=200.0, added_space=500.0,
+                         shot_depth=6.0)
+    g = survey.load_was(cfg)
+    ids, pos, bat, lines, spacing = oracle.nav_read_was(nav, 1111, 40, 200.0, 500.0, 12.5)
+    assert np.array_equal(g.pos_shot, pos) and g.lines == lines and g.spacing == spacing
+    bm = oracle.bathymetry_nav(pos, bat, 2600.0, 209, 12.5)
+    assert np.array_equal(g.bat_model, bm)
+    oid, px, pz, gx, gz = oracle.nav_read_obs(obs, 3, 12.5)
+    pz_r, gz_r = oracle.relocate_obs(gx, bm, 12.5)
+    for i in range(3):
+        zrow = gz[i] if i == 0 else gz_r[i]   # the first OBS keeps its navigation depth
+        want = oracle.geometry_was(int(gx[i]), int(zrow), pos, 6.0, 12.5)
+        assert (g.nxSou[i], g.nySou[i]) == want[:2]
+        assert np.array_equal(g.nxRec[i], want[2]) and np.array_equal(g.nyRec[i], want[3])
+    assert np.array_equal(g.pos_zobs, pz_r) and np.array_equal(g.zgrid, gz_r)
+    s = survey.was_inputs(cfg, g, 2)
+    assert s["obs_id"] == 2 and np.array_equal(s["Field_Data"], gathers[1][:, :NT])
