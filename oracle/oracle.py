@@ -133,6 +133,7 @@ def solver(iprop: int, *, dPML: int, fs: int, nxSou, nySou, nxRec, nyRec, S, dmo
     vp = _f32(vp)
     nx, ny = vp.shape
     nrec = len(np.atleast_1d(nxRec))
+    _check_geometry(nxSou, nySou, nxRec, nyRec, nx, ny)
     S = _f32(S).reshape(-1)
     if Fields is None:
         Fields = np.zeros((nt_snap, nx, ny), dtype=dtype)
@@ -164,6 +165,18 @@ def forward_dump_p(*, dPML, fs, nxSou, nySou, nxRec, nyRec, S, dmodel, dt, vp, n
     return pd
 
 
+def _check_geometry(nxSou, nySou, nxRec, nyRec, nx, ny):
+    """The restatement indexes its arrays with the geometry as the reference
+    does, without checks: refuse a source or receivers outside the grid
+    (1-based, nx columns by ny rows) rather than read or write outside the
+    arrays."""
+    xs, ys = np.atleast_1d(nxSou), np.atleast_1d(nySou)
+    xr, yr = np.atleast_1d(nxRec), np.atleast_1d(nyRec)
+    if (xs.min() < 1 or xs.max() > nx or ys.min() < 1 or ys.max() > ny or
+            (xr.size and (xr.min() < 1 or xr.max() > nx or yr.min() < 1 or yr.max() > ny))):
+        raise ValueError(f"source or receivers outside the {nx} x {ny} grid")
+
+
 def rtm_shot(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target,
              dd: float, dt: float, nx: int, vp_w, added_space: float, store_snap: int, nt_snap: int,
              nt_prop2: int, nt_taper: int, taper_option: int = 0, N_taper: int = 1, N_zeros: int = 0,
@@ -173,6 +186,7 @@ def rtm_shot(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, Data_s
     vp_w = _f32(vp_w)
     nx_w, ny = vp_w.shape
     nrec = len(np.atleast_1d(nxRec))
+    _check_geometry(nxSou, nySou, nxRec, nyRec, nx, ny)  # model coordinates
     img = np.zeros((nx_w, ny), dtype=dtype)
     synth = np.zeros((nrec, nt_prop2), dtype=dtype) if want_synth else None
     fn = lib().orc_rtm_shot_f if dtype == np.float32 else lib().orc_rtm_shot_d
@@ -195,6 +209,7 @@ def rtm_shot_mixed(*, dPML: int, fs: int, nxSou: int, nySou: int, nxRec, nyRec, 
     asked, the snapshots as read back (nsnap, nx_w, ny)."""
     vp_w = _f32(vp_w)
     nx_w, ny = vp_w.shape
+    _check_geometry(nxSou, nySou, nxRec, nyRec, nx, ny)  # model coordinates
     nrec = len(np.atleast_1d(nxRec))
     nsnap = (nt_prop2 - 1) // store_snap
     img = np.zeros((nx_w, ny), dtype=dtype)

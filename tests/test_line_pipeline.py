@@ -30,7 +30,8 @@ def line(tmp_path, oracle):
         nxr = (1 + np.floor(pos_rec / np.float32(DD))).astype(np.int32)
         nyr = np.full(NREC, 2, np.int32)
         nx_w, x_i, x_f = oracle.dynamic_window(nxs, nxr, DD, NX, 100.0)
-        _, obs = oracle.rtm_shot(dPML=DPML, fs=0, nxSou=nxs - x_i + 1, nySou=2, nxRec=nxr - x_i + 1, nyRec=nyr,
+        # rtm_shot takes model coordinates and the window's slice of the model
+        _, obs = oracle.rtm_shot(dPML=DPML, fs=0, nxSou=nxs, nySou=2, nxRec=nxr, nyRec=nyr,
                                  Data_source=src, Data_target=np.zeros((NREC, NT), np.float32), dd=DD, dt=DT,
                                  nx=NX, vp_w=np.ascontiguousarray(vel[x_i - 1:x_f]), added_space=100.0,
                                  store_snap=1, nt_snap=NT, nt_prop2=NT, nt_taper=NT, want_synth=True)
@@ -45,11 +46,14 @@ def test_marine_line_on_the_host(engine_lib, oracle, line, tmp_path):
     from psdm_b200 import driver, rtm, survey
     from psdm_b200._lib import Conditioning
     tmp, vel, src, paths = line
+    # positions along the line start at d_shot_model for the first shot: 600 m,
+    # where the gathers above were modelled
     cfg = survey.McsLine(nav_path=str(tmp / "nav.txt"), su_paths=paths, num_rec=NREC, ns_max=NS_MAX, nt=NT, dt=DT,
-                         dd=DD, cols=11, dir_boat=1, shot_depth=10.0, streamer_depth=10.0, offset_header=0,
-                         near_offset=40.0, drec=20.0)
+                         dd=DD, cols=11, dir_boat=1, d_shot_model=600.0, shot_depth=10.0, streamer_depth=10.0,
+                         offset_header=0, near_offset=40.0, drec=20.0)
     geom = survey.load_line(cfg)
     assert (geom.line_i, geom.line_f) == (1, 4)
+    assert all(r.min() >= 1 for r in geom.nxRec) and max(geom.nxSou) <= NX
     bat = rtm.batmodel_from_velocity(vel, DD, 1500.0)
     cond = Conditioning(0, 0, 0, 0.0, 0.0)
     windows = {}
@@ -61,8 +65,8 @@ def test_marine_line_on_the_host(engine_lib, oracle, line, tmp_path):
         tgt = oracle.condition_traces(cut_multiple=0, cut_sf=0, taper_option=0, Field_Data=s["Field_Data"],
                                       dt_data=DT, dt_prop=DT, nt_prop2=int(lens[0]), nt_taper=int(lens[1]),
                                       N_taper=int(lens[2]), N_zeros=int(lens[3]), nt_cut=cut, nt_sf=sf)
-        img = oracle.rtm_shot(dPML=DPML, fs=0, nxSou=s["nxSou"] - x_i + 1, nySou=s["nySou"],
-                              nxRec=s["nxRec"] - x_i + 1, nyRec=s["nyRec"], Data_source=src, Data_target=tgt, dd=DD,
+        img = oracle.rtm_shot(dPML=DPML, fs=0, nxSou=s["nxSou"], nySou=s["nySou"],
+                              nxRec=s["nxRec"], nyRec=s["nyRec"], Data_source=src, Data_target=tgt, dd=DD,
                               dt=DT, nx=NX, vp_w=np.ascontiguousarray(vel[x_i - 1:x_f]), added_space=100.0,
                               store_snap=1, nt_snap=int(lens[1]), nt_prop2=int(lens[0]), nt_taper=int(lens[1]))
         windows[icount] = (img, x_i, x_f)
