@@ -339,6 +339,10 @@ int psdm_condition_traces_device(psdm_engine* e, const psdm_conditioning* c, int
  */
 int psdm_freq_filter(psdm_engine* e, float* traces, int32_t nt, float dt, int32_t Num, int32_t typef,
                      float f1, float f2);
+/* The filter's response H (ts complex values, interleaved re/im) for sampling
+ * frequency fe = 1/dt and zero-padded length ts (24 nt), as butterworth
+ * computes it (src/filters.f90:129-232); host only. */
+int psdm_butterworth_response(int32_t ts, float fe, int32_t typef, float f1, float f2, float* H);
 /* Same on a device array; asynchronous on the engine's stream. */
 int psdm_freq_filter_device(psdm_engine* e, float* d_traces, int32_t nt, float dt, int32_t Num,
                             int32_t typef, float f1, float f2);

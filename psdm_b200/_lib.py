@@ -25,7 +25,7 @@ EXPORTS = [
     "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
     "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
     "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch",
-    "psdm_freq_filter", "psdm_freq_filter_device",
+    "psdm_freq_filter", "psdm_freq_filter_device", "psdm_butterworth_response",
     "psdm_nav_read", "psdm_channel_positions", "psdm_geometry_mcs", "psdm_linear_2d", "psdm_batmodel_from_velocity",
     "psdm_nav_read_was", "psdm_nav_read_obs", "psdm_geometry_was", "psdm_bathymetry_nav", "psdm_relocate_obs",
 ]
@@ -109,6 +109,7 @@ def lib():
     L.psdm_su_write_image.argtypes = [C.c_char_p, _I, _I, _F, _F, _I, _f32p, _I]
     L.psdm_su_read_shot.argtypes = [C.c_char_p, _I, _I, _I, _I, _I, _f32p, _P]
     L.psdm_su_read_header_i32.argtypes = [C.c_char_p, _I, _I, _I, _I, _i32p]
+    L.psdm_butterworth_response.argtypes = [_I, _F, _I, _F, _F, _f32p]
     L.psdm_nav_read.argtypes = [C.c_char_p, _I, _I, _F, _I, _I, _I, _P, _P, _P, _i32p]
     L.psdm_channel_positions.argtypes = [_F, _I, _I, _I, _F, _P, _F, _F, _f32p]
     L.psdm_geometry_mcs.argtypes = [_F, _I, _f32p, _F, _F, _F, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _i32p,

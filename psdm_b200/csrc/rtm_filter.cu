@@ -16,6 +16,7 @@
 #include <complex>
 #include <vector>
 
+#include "../../include/psdm_rtm.h"
 #include "rtm_internal.h"
 
 namespace psdm {
@@ -142,3 +143,12 @@ void destroy_fft_plans(int* plans) {
 }
 
 }  // namespace psdm
+
+extern "C" int psdm_butterworth_response(int32_t ts, float fe, int32_t typef, float f1, float f2, float* H) {
+    if (!H || ts < 2 || (ts & 1) || typef < 1 || typef > 3) {
+        psdm::set_last_error("psdm_butterworth_response: null output, odd or short length, or typef not 1..3");
+        return PSDM_ERR_ARG;
+    }
+    psdm::butterworth_response(ts, fe, typef, f1, f2, reinterpret_cast<std::complex<float>*>(H));
+    return PSDM_OK;
+}

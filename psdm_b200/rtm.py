@@ -328,6 +328,13 @@ def su_read_header_i32(path: str, nrec: int, ns_max: int, byte_pos: int, big_end
     return out
 
 
+def butterworth_response(ts: int, fe: float, typef: int, f1: float, f2: float) -> np.ndarray:
+    """psdm_butterworth_response: the frequency filter's response H (ts,) complex64."""
+    out = np.zeros(2 * ts, np.float32)
+    L.check(L.lib().psdm_butterworth_response(ts, fe, typef, f1, f2, out))
+    return out.view(np.complex64)
+
+
 def nav_read(path: str, cols: int, dir_boat: int, d_shot_model: float, shot_i: int = 0, shot_f: int = 0):
     """psdm_nav_read: (shotID, pos_shot, pos_bat, line_i, line_f) of a shot navigation file."""
     out = np.zeros(3, np.int32)

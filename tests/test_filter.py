@@ -60,3 +60,23 @@ def test_zero_traces_untouched(oracle):
     out = oracle.freq_filter(x, 1e-3, 1, 0.0, 25.0)
     assert np.all(out[0] == 0) and np.all(out[2] == 0) and np.any(out[1] != 0)
     assert np.array_equal(oracle.freq_filter(np.zeros((2, 9)), 1e-3, 3, 5.0, 30.0), np.zeros((2, 9)))
+
+
+@pytest.mark.parametrize("typef,f1,f2", [(1, 0.0, 25.0), (2, 0.0, 30.0), (3, 5.0, 40.0)])
+@pytest.mark.parametrize("ts,fe", [(24 * 750, 250.0), (24 * 1001, 500.0)])
+def test_engine_response_matches_oracle(engine_lib, oracle, typef, f1, f2, ts, fe):
+    """The engine computes the response on the host in single precision in
+    the reference's order.  Its complex arithmetic (C++ std::complex) and
+    cosine differ from numpy's in the last bits of each operation, so against
+    the oracle's restatement the bar is 1e-5 of the response's largest value
+    (about 10 ulp accumulated over the three section products and the
+    division), ten times inside the filter's own 1e-4."""
+    from psdm_b200 import rtm
+    got = rtm.butterworth_response(ts, fe, typef, f1, f2)
+    want = oracle.butterworth_response(ts, fe, typef, f1, f2)
+    assert got.shape == want.shape
+    assert got[0] == want[0]
+    half = ts // 2 + 1
+    err = np.abs(got[:half] - want[:half]).max()
+    assert err <= 1e-5 * np.abs(want).max(), err
+    assert np.array_equal(got[half:], np.conj(got[1:ts - half + 1][::-1]))
