@@ -244,11 +244,14 @@ int psdm_model_shot(
  * d_Data_source (nt), d_Vp_w (ny, nx_w) and d_Data_synth ((nt, NumRec),
  * overwritten) are device pointers owned by the caller; nxRec/nyRec are host
  * arrays.  Work is queued on `stream` (a cudaStream_t; NULL = the legacy
- * default stream) and the call returns when it has finished.  The first call
- * on a device looks up the scratch's device address and prepares the
- * kernels; make it before any stream capture begins.  All calls on a device
- * share the one scratch: calls that overlap on the GPU (other host threads,
- * or other streams) race and corrupt each other's results.
+ * default stream) and the call returns when it has finished.  Every call
+ * looks up the scratch's device address in the context current at the call
+ * (the first call on a device also prepares the kernels).  The call copies
+ * from pageable host memory and waits for `stream`, so it must not be made
+ * while `stream`, or any other stream of the device, is being captured into
+ * a CUDA graph.  All calls on a device share the one scratch: calls that
+ * overlap on the GPU (other host threads, or other streams) race and corrupt
+ * each other's results.
  */
 int psdm_model_shot_noalloc(
     const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,

@@ -216,15 +216,7 @@ int check_params(const psdm_params* prm) {
 
 int build_grid(const psdm_params* prm, int ny, int nx, Grid* g) {
     if (ny < 1 || nx < 1) return fail(PSDM_ERR_ARG, "grid must be at least 1x1 (ny=%d nx=%d)", ny, nx);
-    g->ny = ny;
-    g->nx = nx;
-    g->dPML = prm->dPML;
-    g->dn = prm->dPML + 2 * kAcc;
-    g->nyt = g->dn + ny + g->dn;
-    g->nxt = nx + 2 * g->dn;
-    g->zoff = (4 - g->dn % 4) % 4;
-    g->ldz = (g->zoff + g->nyt + 31) / 32 * 32;
-    g->ldf = (ny + 3) / 4 * 4;
+    *g = make_grid(prm->dPML, ny, nx);
     return PSDM_OK;
 }
 
@@ -704,9 +696,7 @@ int sync(psdm_engine* e) {
     if (e->h_err && *e->h_err) {
         const int code = *e->h_err;
         *e->h_err = 0;
-        if (code == 2) return fail(PSDM_ERR_CUDA, "a step kernel was given a tile plan for another launch form");
-        if (code == 3) return fail(PSDM_ERR_CUDA, "a pass kernel timed out waiting for neighbouring tiles");
-        return fail(PSDM_ERR_CUDA, "a step kernel timed out waiting for its shared-memory copies");
+        return fail(PSDM_ERR_CUDA, "%s", step_error_message(code));
     }
     return PSDM_OK;
 }

@@ -32,6 +32,34 @@ struct Grid {
     size_t field_cells() const { return (size_t)ldf * (size_t)nx; }
 };
 
+// The layout above for an ny x nx window and a C-PML of dPML cells (ny, nx,
+// dPML >= 1).  Every path that builds a padded grid uses this one function.
+inline Grid make_grid(int dPML, int ny, int nx) {
+    Grid g;
+    g.ny = ny;
+    g.nx = nx;
+    g.dPML = dPML;
+    g.dn = dPML + 2 * kAcc;
+    g.nyt = g.dn + ny + g.dn;
+    g.nxt = nx + 2 * g.dn;
+    g.zoff = (4 - g.dn % 4) % 4;
+    g.ldz = (g.zoff + g.nyt + 31) / 32 * 32;
+    g.ldf = (ny + 3) / 4 * 4;
+    return g;
+}
+
+// Message for a nonzero value of a step kernel's error word: 1 = a bounded
+// wait for the tile's shared-memory copies ran out, 2 = the tile plan was
+// made for another launch form, 3 = a pass kernel gave up waiting for its
+// neighbouring tiles.
+inline const char* step_error_message(int code) {
+    switch (code) {
+        case 2: return "a step kernel was given a tile plan for another launch form";
+        case 3: return "a pass kernel timed out waiting for neighbouring tiles";
+        default: return "a step kernel timed out waiting for its shared-memory copies";
+    }
+}
+
 // Arguments of one fused time step.  Pointers are device pointers.
 struct StepArgs {
     // wavefield: p = level n (read only); pm = level n-1 in, level n+1 out

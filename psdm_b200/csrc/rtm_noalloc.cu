@@ -20,11 +20,14 @@
 // (rtm_step.cu), so the traces are identical to psdm_model_shot's.
 //
 // In host code the name g_noalloc_scratch stands for the host-side shadow
-// of the variable, not for device memory: its device address is looked up
-// once per device with cudaGetSymbolAddress (with that device current) and
-// that address is what the kernels receive.  The first call on a device
-// does that look-up and sets the step kernels' attributes; make that first
-// call before any stream capture begins.
+// of the variable, not for device memory: every call looks its device
+// address up with cudaGetSymbolAddress, with the caller's device current,
+// and hands that address to the kernels.  The address belongs to the CUDA
+// context current at the call, so a device reset or another context
+// between calls is harmless.  The first call on a device also sets the
+// step kernels' attributes.  The call copies from pageable host memory and
+// waits for its stream, so it must not be made while any stream of the
+// device is being captured into a CUDA graph.
 
 #include <cuda_runtime.h>
 
@@ -75,27 +78,31 @@ int nfail(int code, const char* fmt, ...) {
         if (e_ != cudaSuccess) return nfail(PSDM_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
     } while (0)
 
-// Per-device set-up, done by the first call on each device.
+// Kernel attributes are set once per device; the scratch's device address
+// is looked up on every call (a cheap driver query), so that it always
+// belongs to the context current at the call.
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-unsigned char* g_scratch_addr[kMaxDevices] = {nullptr};
+bool g_prepared[kMaxDevices] = {false};
 
 int scratch_address(int dev, unsigned char** out) {
     if (dev < 0 || dev >= kMaxDevices) return nfail(PSDM_ERR_ARG, "device ordinal %d not supported", dev);
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        // Step kernel attributes (shared-memory size), then the scratch's
-        // device address; the look-up also loads this library's device code
-        // on the device if that has not happened yet.
-        const int rc = prepare_step_kernels();
-        if (rc) return nfail(PSDM_ERR_CUDA, "preparing the step kernels: %s", cudaGetErrorString((cudaError_t)rc));
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr)
-            return nfail(PSDM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array: %s", cudaGetErrorString(e));
-        g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+    {
+        std::lock_guard<std::mutex> lk(g_setup_mu);
+        if (!g_prepared[dev]) {
+            const int rc = prepare_step_kernels();
+            if (rc)
+                return nfail(PSDM_ERR_CUDA, "preparing the step kernels: %s", cudaGetErrorString((cudaError_t)rc));
+            g_prepared[dev] = true;
+        }
     }
-    *out = g_scratch_addr[dev];
+    // The look-up also loads this library's device code into the current
+    // context if that has not happened yet.
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+        return nfail(PSDM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array: %s", cudaGetErrorString(e));
+    *out = static_cast<unsigned char*>(ptr);
     return PSDM_OK;
 }
 
@@ -148,16 +155,9 @@ extern "C" int psdm_model_shot_noalloc(const psdm_params* prm, int32_t NumRec, i
         return nfail(PSDM_ERR_ARG, "need NumRec >= 1, nt >= 2 and a non-empty window");
 
     // Padded grid of the window, laid out as the engine lays it out.
-    Grid g;
-    g.ny = ny;
-    g.nx = nx_w;
-    g.dPML = prm->dPML;
-    g.dn = prm->dPML + 2 * kAcc;
-    g.nyt = g.dn + ny + g.dn;
-    g.nxt = nx_w + 2 * g.dn;
-    g.zoff = (4 - g.dn % 4) % 4;
-    g.ldz = (g.zoff + g.nyt + 31) / 32 * 32;
-    g.ldf = (ny + 3) / 4 * 4;
+    if (prm->dPML > kMaxDn - 2 * kAcc)
+        return nfail(PSDM_ERR_ARG, "dPML %d too large for the fixed scratch (max %d)", prm->dPML, kMaxDn - 2 * kAcc);
+    const Grid g = make_grid(prm->dPML, ny, nx_w);
     if (prm->strategy == 1 && nx_w < g.dn)
         return nfail(PSDM_ERR_ARG, "RAM ordering needs nx_w >= dPML+6 (nx_w=%d, dPML=%d)", nx_w, prm->dPML);
     if (g.dn > kMaxDn || g.cells() > kMaxCells || g.ldz > kMaxRows || g.nxt > kMaxCols || NumRec > kMaxRec)
@@ -313,6 +313,6 @@ extern "C" int psdm_model_shot_noalloc(const psdm_params* prm, int32_t NumRec, i
     int herr = 0;
     NA_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     NA_CUDA(cudaStreamSynchronize(st));
-    if (herr) return nfail(PSDM_ERR_CUDA, "a step kernel timed out waiting for its shared-memory copies");
+    if (herr) return nfail(PSDM_ERR_CUDA, "%s", step_error_message(herr));
     return PSDM_OK;
 }

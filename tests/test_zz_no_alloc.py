@@ -83,6 +83,48 @@ def test_noalloc_same_shot_twice(engine):
     _assert_same(second, want, "second call")
 
 
+def _noalloc_prepared(c):
+    """Device buffers made first, so that the call itself is all that runs
+    between two readings of the free device memory."""
+    import torch
+    from psdm_b200 import _lib as L
+    dev = torch.device("cuda", 0)
+    src = torch.from_numpy(np.ascontiguousarray(c["src"], dtype=np.float32)).to(dev)
+    vp = torch.from_numpy(np.ascontiguousarray(c["vp_w"], dtype=np.float32)).to(dev)
+    nrec = int(c["nxRec"].size)
+    out = torch.zeros((nrec, c["nt"]), dtype=torch.float32, device=dev)
+    nxr = np.ascontiguousarray(c["nxRec"], dtype=np.int32)
+    nyr = np.ascontiguousarray(c["nyRec"], dtype=np.int32)
+    prm = _prm(c).c()
+    stream = torch.cuda.current_stream(dev)
+
+    def call():
+        L.check(L.lib().psdm_model_shot_noalloc(
+            C.byref(prm), nrec, int(c["nxSou"]), int(c["nySou"]), nxr, nyr, src.data_ptr(), c["dd"], c["dt"],
+            c["ny"], c["nx"], c["nx_w"], vp.data_ptr(), c["added_space"], c["nt"], out.data_ptr(),
+            stream.cuda_stream))
+    return call, out
+
+
+def test_noalloc_allocates_nothing(engine):
+    # After one call on a shot, a call on a different (larger) shot must not
+    # change the device's free memory: the scratch is static.
+    import torch
+    a = make_case(fs=1, nt=120, seed=21)
+    b = make_case(ny=150, nx_model=420, nt=90, dPML=11, fs=0, strategy=2, nrec=60, rec_step=3, sou_x=300,
+                  sou_z=5, rec_z=3, added_space=150.0, seed=22)
+    call_a, _ = _noalloc_prepared(a)
+    call_b, out_b = _noalloc_prepared(b)
+    call_a()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    call_b()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes across the call"
+    _assert_same(out_b.cpu().numpy(), _engine_traces(engine, b), "traces")
+
+
 def test_noalloc_rejects_oversized_shot(engine):
     from psdm_b200._lib import PsdmError
     # A 2000 x 242 window pads to 2048 x 270 cells, above the 2^19-cell scratch.
