@@ -205,6 +205,17 @@ int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval);
  * mixed-precision snapshot conversion always use one launch per step.
  */
 int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on);
+/*
+ * Time steps per kernel launch for every pass of the engine (no reference
+ * counterpart; the reference advances its arrays one step at a time,
+ * solver_ac_forward_ram.f90:344-573): 2 (default) advances each tile two
+ * steps per launch, level n+1 computed on the tile and a 3-cell ring in
+ * shared memory, so that the wavefield crosses HBM and the launch queue half
+ * as often; 1 launches one kernel per step.  Same results bit for bit.  The
+ * cooperative pass launch (psdm_engine_set_pass_launch) and checkpointed
+ * shots use one step per launch.
+ */
+int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps);
 
 /* Shots in flight at a time in the last batched call. */
 int32_t psdm_engine_batch_slots(const psdm_engine* e);

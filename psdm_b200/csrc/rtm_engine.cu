@@ -82,6 +82,13 @@ struct psdm_engine {
         cudaGraphExec_t exec = nullptr;
     } graphs[3];
     bool use_graphs = true;
+    // Time steps per launch: 2 = pair launches (rtm_pair.cu), 1 = one launch
+    // per step.  Captured pair loops, one per pass kind.
+    int steps_per_launch = 2;
+    struct PairGraphCache {
+        std::vector<PairArgs> args;
+        cudaGraphExec_t exec = nullptr;
+    } pgraphs[3];
     // Passes of one shot as one cooperative launch each (pass_kernel) where
     // the pass allows it; the neighbour and receiver lists of the last plan
     // of each pass kind stay on the device while the plan (key) is unchanged.
@@ -156,6 +163,11 @@ struct psdm_engine {
             g.exec = nullptr;
             g.args.clear();
         }
+        for (auto& g : pgraphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            g.args.clear();
+        }
     }
     // Profiling marks: 0 = shot start, 1 = forward done, 2 = backward done.
     int record(int which) {
@@ -180,13 +192,18 @@ struct Shot {
     Grid g;
     float dt = 0.f, dd = 0.f;
     int fs = 0, disk = 0;
-    float* p[2] = {nullptr, nullptr};
+    // p[0], p[1]: the two levels of one launch per step (p1 overwritten in
+    // place); p[2] and p[3] for launches of two steps, whose wavefield
+    // rotates through all four.
+    float* p[4] = {nullptr, nullptr, nullptr, nullptr};
     float* c2 = nullptr;
     float* phx[2] = {nullptr, nullptr};
     float* chx = nullptr;
+    float* chx2 = nullptr;  // second chi buffers (launches of two steps)
     float* phz[2] = {nullptr, nullptr};
     float* chz = nullptr;
-    float* side[2] = {nullptr, nullptr};
+    float* chz2 = nullptr;
+    float* side[4] = {nullptr, nullptr, nullptr, nullptr};
     float* fA = nullptr;
     float* fB = nullptr;
     float cf1[4], cf2[4];
@@ -223,10 +240,10 @@ int build_grid(const psdm_params* prm, int ny, int nx, Grid* g) {
 // Zero the wavefield, memory variables and free-surface histories.
 int reset_state(psdm_engine* e, Shot* s) {
     const size_t n = s->g.cells();
-    for (float* b : {s->p[0], s->p[1], s->phx[0], s->phx[1], s->chx, s->phz[0], s->phz[1], s->chz})
+    for (float* b : {s->p[0], s->p[1], s->p[2], s->p[3], s->phx[0], s->phx[1], s->chx, s->chx2, s->phz[0], s->phz[1],
+                     s->chz, s->chz2})
         CUDA_TRY(cudaMemsetAsync(b, 0, n * sizeof(float), e->stream));
-    CUDA_TRY(cudaMemsetAsync(s->side[0], 0, s->g.nxt * sizeof(float), e->stream));
-    CUDA_TRY(cudaMemsetAsync(s->side[1], 0, s->g.nxt * sizeof(float), e->stream));
+    for (float* b : s->side) CUDA_TRY(cudaMemsetAsync(b, 0, s->g.nxt * sizeof(float), e->stream));
     CUDA_TRY(cudaMemsetAsync(s->counters, 0, 2 * sizeof(int), e->stream));
     return PSDM_OK;
 }
@@ -247,17 +264,18 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
     s->fs = prm->fs != 0;
     s->disk = prm->strategy == 2;
     const size_t n = g.cells();
-    TRY(e->get(("p0" + tag).c_str(), n, &s->p[0]));
-    TRY(e->get(("p1" + tag).c_str(), n, &s->p[1]));
+    for (int i = 0; i < 4; ++i) TRY(e->get(("p" + std::to_string(i) + tag).c_str(), n, &s->p[i]));
     TRY(e->get(("c2" + tag).c_str(), n, &s->c2));
     TRY(e->get(("phx0" + tag).c_str(), n, &s->phx[0]));
     TRY(e->get(("phx1" + tag).c_str(), n, &s->phx[1]));
     TRY(e->get(("chx" + tag).c_str(), n, &s->chx));
+    TRY(e->get(("chx2" + tag).c_str(), n, &s->chx2));
     TRY(e->get(("phz0" + tag).c_str(), n, &s->phz[0]));
     TRY(e->get(("phz1" + tag).c_str(), n, &s->phz[1]));
     TRY(e->get(("chz" + tag).c_str(), n, &s->chz));
-    TRY(e->get(("side0" + tag).c_str(), (size_t)g.nxt, &s->side[0]));
-    TRY(e->get(("side1" + tag).c_str(), (size_t)g.nxt, &s->side[1]));
+    TRY(e->get(("chz2" + tag).c_str(), n, &s->chz2));
+    for (int i = 0; i < 4; ++i)
+        TRY(e->get(("side" + std::to_string(i) + tag).c_str(), (size_t)g.nxt, &s->side[i]));
     TRY(e->get(("fA" + tag).c_str(), (size_t)g.dn, &s->fA));
     TRY(e->get(("fB" + tag).c_str(), (size_t)g.dn, &s->fB));
     TRY(e->get(("tile_counters" + tag).c_str(), 2, &s->counters));
@@ -555,6 +573,227 @@ int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args, in
     return PSDM_OK;
 }
 
+// Buffers of the mixed-precision form (see below): FP32 staging of the
+// snapshots (slot m in stage[m % 4]; a snapshot is converted by the launch
+// after the one that stages it, and a launch of two steps may stage two),
+// 16-bit snapshots with their scales, and the image's Kahan compensation.
+struct MixedBufs {
+    int kind = 0;  // 1 binary16, 2 bfloat16
+    int ks = 1;    // snapshot interval (store_snap)
+    int nsnap = 0;
+    size_t fstride = 0;
+    float* stage[4] = {nullptr, nullptr, nullptr, nullptr};
+    unsigned int* amax = nullptr;  // nsnap
+    unsigned short* snap16 = nullptr;  // nsnap * fstride
+    float* iscale = nullptr;       // nsnap
+    float* comp = nullptr;         // fstride
+};
+
+// ---- two steps per launch -------------------------------------------------
+//
+// A pass of pair launches (rtm_pair.cu) is made from the pass's one-step
+// arguments: the kernels need the per-step values of one or two steps, the
+// shot's buffers rotated as the levels advance, and a tile plan of their own.
+
+bool pair_on(const psdm_engine* e) { return e->steps_per_launch == 2 && !e->use_pass; }
+
+// Rotation of a shot's buffers through a pass of pair launches.  At the
+// first step of a pass the one-step launches read p = p[0] (level n), p1 =
+// p[1], phi from phx[0] / phz[0], chi from chx / chz and the free-surface
+// histories side[0] (level n) and side[1]; pair launches start from the
+// same state and write to the other buffers.
+struct PairRot {
+    float* prev;   // level n-1
+    float* cur;    // level n
+    float* fr[2];  // free: levels n+1, n+2
+    float *phx_in, *phx_out, *phz_in, *phz_out;
+    float *chx_in, *chx_out, *chz_in, *chz_out;
+    float* sprev;
+    float* scur;
+    float* sfr[2];
+};
+
+PairRot pair_rot_start(const Shot& s) {
+    return PairRot{s.p[1],   s.p[0], {s.p[2], s.p[3]}, s.phx[0],  s.phx[1],  s.phz[0], s.phz[1],
+                   s.chx,    s.chx2, s.chz,            s.chz2,    s.side[1], s.side[0], {s.side[2], s.side[3]}};
+}
+
+void pair_rot_advance(PairRot& r, int nsub) {
+    if (nsub == 2) {
+        std::swap(r.prev, r.fr[0]);
+        std::swap(r.cur, r.fr[1]);
+        std::swap(r.sprev, r.sfr[0]);
+        std::swap(r.scur, r.sfr[1]);
+    } else {
+        float* t = r.prev;
+        r.prev = r.cur;
+        r.cur = r.fr[0];
+        r.fr[0] = t;
+        t = r.sprev;
+        r.sprev = r.scur;
+        r.scur = r.sfr[0];
+        r.sfr[0] = t;
+    }
+    std::swap(r.phx_in, r.phx_out);
+    std::swap(r.phz_in, r.phz_out);
+    std::swap(r.chx_in, r.chx_out);
+    std::swap(r.chz_in, r.chz_out);
+}
+
+// Pair launches for the one-step arguments steps[first, first + count) of a
+// pass of mode `mode` (step k = i - first + 2).  row_slot: the host copy of
+// the pass's injection row map.  Forward passes with receivers gather them
+// inside the tiles (h_rec_cell: the receivers' cells, nrec of them).  mb:
+// the mixed form's buffers for a forward pass, whose snapshot conversions
+// move to the launch after the one that stages the snapshot, or null.
+// Out: the launches, the buffer holding the pass's last level, and the
+// snapshot slots staged by the last launch (to be converted after the pass).
+int make_pairs(psdm_engine* e, const Shot& s, int mode, const std::vector<StepArgs>& steps, size_t first,
+               size_t count, const std::vector<int>& row_slot, int nrec, const int* h_rec_cell, const MixedBufs* mb,
+               const std::string& tag, std::vector<PairArgs>* out, float** last, std::vector<int>* pending) {
+    PairRot r = pair_rot_start(s);
+    *last = r.cur;
+    if (pending) pending->clear();
+    if (count == 0) return PSDM_OK;
+    PairArgs base;
+    std::memset(&base, 0, sizeof(base));
+    base.a = steps[first];
+    if (!plan_pair(&base, row_slot.empty() ? nullptr : row_slot.data()))
+        return fail(PSDM_ERR_ARG, "the tile plan of the two-step launches needs more than %d rectangles", kPairRects);
+    const bool recs = mode == 0 && base.a.rec_out != nullptr && base.a.nrec > 0;
+    if (recs) {
+        std::vector<int> f, ix;
+        pair_rec_lists(base, nrec, h_rec_cell, &f, &ix);
+        int *d_f = nullptr, *d_i = nullptr;
+        TRY(e->get(("pair_recf" + tag).c_str(), f.size(), &d_f));
+        TRY(e->get(("pair_reci" + tag).c_str(), std::max<size_t>(ix.size(), 1), &d_i));
+        CUDA_TRY(cudaMemcpyAsync(d_f, f.data(), f.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        if (!ix.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_i, ix.data(), ix.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));  // the host lists go out of scope
+        base.rec_first = d_f;
+        base.rec_idx = d_i;
+    }
+    std::vector<int> pend;  // slots staged by the previous launch
+    const size_t end = first + count;
+    int sel = 0;
+    out->reserve(out->size() + (count + 1) / 2);
+    for (size_t i = first; i < end;) {
+        const int ns = end - i >= 2 ? 2 : 1;
+        PairArgs q = base;
+        q.a = steps[i];
+        q.a.counter_sel = sel;
+        sel ^= 1;
+        q.a.pm = r.prev;
+        q.a.p = r.cur;
+        q.p_out[0] = r.fr[0];
+        q.p_out[1] = r.fr[1];
+        q.a.phix_in = r.phx_in;
+        q.a.phix_out = r.phx_out;
+        q.a.phiz_in = r.phz_in;
+        q.a.phiz_out = r.phz_out;
+        q.chix_in = r.chx_in;
+        q.a.chix = r.chx_out;
+        q.chiz_in = r.chz_in;
+        q.a.chiz = r.chz_out;
+        q.a.side_pm = r.sprev;
+        q.a.side_p = r.scur;
+        q.side_out[0] = r.sfr[0];
+        q.side_out[1] = r.sfr[1];
+        q.nsub = ns;
+        for (int j = 0; j < ns; ++j) {
+            const StepArgs& t = steps[i + j];
+            SubStep& u = q.sub[j];
+            u.field = t.field;
+            u.field16 = t.field16;
+            u.field_iscale = t.field_iscale;
+            u.field_amax = t.field_amax;
+            u.field_w = t.field_w;
+            u.inj_t = t.inj_t;
+            u.rec_t = recs ? (int)(i + j - first) : -1;  // step k gives Rec(k-1)
+        }
+        q.a.q_src = nullptr;
+        q.q_src2 = nullptr;
+        if (mb) {
+            for (size_t k = 0; k < pend.size() && k < 2; ++k) {
+                const int m = pend[k];
+                const float* src = mb->stage[m & 3];
+                const unsigned int* am = mb->amax + (m - 1);
+                void* dst = mb->snap16 + (size_t)(m - 1) * mb->fstride;
+                float* isc = mb->iscale + (m - 1);
+                if (k == 0) {
+                    q.a.q_n = (int)mb->fstride;
+                    q.a.q_src = src;
+                    q.a.q_amax = am;
+                    q.a.q_dst = dst;
+                    q.a.q_iscale = isc;
+                } else {
+                    q.q_n2 = (int)mb->fstride;
+                    q.q_src2 = src;
+                    q.q_amax2 = am;
+                    q.q_dst2 = dst;
+                    q.q_iscale2 = isc;
+                }
+            }
+            pend.clear();
+            for (int j = 0; j < ns; ++j)
+                if (steps[i + j].field_amax != nullptr) pend.push_back((int)(steps[i + j].field_amax - mb->amax) + 1);
+        }
+        out->push_back(q);
+        pair_rot_advance(r, ns);
+        i += ns;
+    }
+    *last = r.cur;
+    if (pending) *pending = pend;
+    return PSDM_OK;
+}
+
+// Launch a pass of pair launches, captured once into a CUDA graph and
+// replayed while the argument list is unchanged (as launch_steps does).
+int launch_pairs(psdm_engine* e, int mode, const std::vector<PairArgs>& L) {
+    if (L.empty()) return PSDM_OK;
+    e->launches += (int64_t)L.size();
+    auto& gc = e->pgraphs[mode];
+    if (e->use_graphs) {
+        const bool same = gc.exec && gc.args.size() == L.size() &&
+                          std::memcmp(gc.args.data(), L.data(), L.size() * sizeof(PairArgs)) == 0;
+        if (!same) {
+            if (gc.exec) cudaGraphExecDestroy(gc.exec);
+            gc.exec = nullptr;
+            gc.args.clear();
+            cudaStream_t cs = e->own_stream;
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                for (const PairArgs& q : L)
+                    if (launch_pair(mode, q, cs) != 0) {
+                        ok = false;
+                        break;
+                    }
+                ok = (cudaStreamEndCapture(cs, &graph) == cudaSuccess) && ok;
+            }
+            if (ok) ok = cudaGraphInstantiate(&gc.exec, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();  // clear a failed capture
+            if (ok) {
+                gc.args = L;
+            } else {
+                gc.exec = nullptr;
+                e->use_graphs = false;
+            }
+        }
+        if (gc.exec) {
+            CUDA_TRY(cudaGraphLaunch(gc.exec, e->stream));
+            return PSDM_OK;
+        }
+    }
+    for (const PairArgs& q : L) {
+        const int rc = launch_pair(mode, q, e->stream);
+        if (rc) return fail(PSDM_ERR_CUDA, "pair launch: %s", cudaGetErrorString((cudaError_t)rc));
+    }
+    return PSDM_OK;
+}
+
 // Step arguments of a forward pass over k = 2..nt
 // (solver_ac_forward_ram.f90:344-577).
 //   d_S: source trace (nt); d_fields: snapshot slots (nslots of ny*nx) or null;
@@ -563,10 +802,11 @@ int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args, in
 //   receiver cells; the per-step arguments are appended to *steps_out.
 int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
                   float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec, const std::string& tag,
-                  std::vector<StepArgs>* steps_out, bool batched = false) {
+                  std::vector<StepArgs>* steps_out, bool batched = false, std::vector<int>* row_slot_out = nullptr) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, 1, &zs, &xs, &inj));
+    if (row_slot_out) *row_slot_out = inj.row_slot;
     int *d_row = nullptr, *d_cols = nullptr;
     TRY(upload_inj(e, g, inj, ("src" + tag).c_str(), &d_row, &d_cols));
     int* d_rec_cell = nullptr;
@@ -610,12 +850,23 @@ int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* 
 int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_S, int zs, int xs,
                 float* d_fields, int nslots, int nrec, const int* h_rec_cell, float* d_rec) {
     std::vector<StepArgs> steps;
-    TRY(build_forward(e, s, nt, store_snap, d_S, zs, xs, d_fields, nslots, nrec, h_rec_cell, d_rec, "", &steps));
+    std::vector<int> row_slot;
+    TRY(build_forward(e, s, nt, store_snap, d_S, zs, xs, d_fields, nslots, nrec, h_rec_cell, d_rec, "", &steps, false,
+                      &row_slot));
     const int* d_rec_cell = steps.empty() ? nullptr : steps[0].rec_cell;
-    TRY(launch_steps(e, 0, steps, nrec, h_rec_cell));
+    const float* pfin = s.p[(nt - 1) & 1];  // p3 of the last step
+    if (pair_on(e)) {
+        std::vector<PairArgs> pairs;
+        float* last = nullptr;
+        TRY(make_pairs(e, s, 0, steps, 0, steps.size(), row_slot, nrec, h_rec_cell, nullptr, "", &pairs, &last,
+                       nullptr));
+        TRY(launch_pairs(e, 0, pairs));
+        pfin = last;
+    } else {
+        TRY(launch_steps(e, 0, steps, nrec, h_rec_cell));
+    }
     e->fwd_steps += nt - 1;
     if (d_rec && nrec > 0 && nt >= 2) {
-        const float* pfin = s.p[(nt - 1) & 1];  // p3 of the last step
         int rc = launch_rec_final(d_rec_cell, pfin, d_rec, nrec, nt, nt, e->stream);
         if (rc) return fail(PSDM_ERR_CUDA, "receiver gather: %s", cudaGetErrorString((cudaError_t)rc));
         e->launches += 1;
@@ -634,10 +885,12 @@ int run_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* d_
 int build_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, const float* d_back, int reverse,
                    int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
                    const float* h_w, float* d_image, const std::string& tag, std::vector<StepArgs>* steps_out,
-                   std::vector<int>* slot_of_step = nullptr, bool batched = false) {
+                   std::vector<int>* slot_of_step = nullptr, bool batched = false,
+                   std::vector<int>* row_slot_out = nullptr) {
     const Grid& g = s.g;
     InjMap inj;
     TRY(build_inj(g, nrec, zr, xr, &inj));
+    if (row_slot_out) *row_slot_out = inj.row_slot;
     int *d_row = nullptr, *d_cols = nullptr;
     TRY(upload_inj(e, g, inj, ("rec" + tag).c_str(), &d_row, &d_cols));
     StepArgs a = base_args(s);
@@ -678,9 +931,17 @@ int run_backward(psdm_engine* e, Shot& s, int nt, int store_snap, int nt_snap, c
                  int nrec, const int* zr, const int* xr, const float* d_fields, int slot_lo, int slot_hi,
                  const float* h_w, float* d_image) {
     std::vector<StepArgs> steps;
+    std::vector<int> row_slot;
     TRY(build_backward(e, s, nt, store_snap, nt_snap, d_back, reverse, nrec, zr, xr, d_fields, slot_lo, slot_hi, h_w,
-                       d_image, "", &steps));
-    TRY(launch_steps(e, 1, steps));
+                       d_image, "", &steps, nullptr, false, &row_slot));
+    if (pair_on(e)) {
+        std::vector<PairArgs> pairs;
+        float* last = nullptr;
+        TRY(make_pairs(e, s, 1, steps, 0, steps.size(), row_slot, 0, nullptr, nullptr, "", &pairs, &last, nullptr));
+        TRY(launch_pairs(e, 1, pairs));
+    } else {
+        TRY(launch_steps(e, 1, steps));
+    }
     e->bwd_steps += nt - 1;
     return PSDM_OK;
 }
@@ -745,33 +1006,19 @@ int window_geometry(const Grid& g, int NumRec, int nxSou, int nySou, const int* 
 // sample store_snap*m.  This form has no reference counterpart; for
 // store_snap = 1 its pairing is the reference's.
 
-struct MixedBufs {
-    int kind = 0;  // 1 binary16, 2 bfloat16
-    int ks = 1;    // snapshot interval (store_snap)
-    int nsnap = 0;
-    size_t fstride = 0;
-    float* stage[2] = {nullptr, nullptr};
-    unsigned int* amax = nullptr;  // nsnap
-    unsigned short* snap16 = nullptr;  // nsnap * fstride
-    float* iscale = nullptr;       // nsnap
-    float* comp = nullptr;         // fstride
-};
-
 int mixed_bufs(psdm_engine* e, const Shot& s, int kind, int ks, int nt_prop2, const std::string& tag, MixedBufs* mb) {
     mb->kind = kind;
     mb->ks = ks;
     mb->nsnap = (nt_prop2 - 1) / ks;
     mb->fstride = s.g.field_cells();
     const size_t fs = mb->fstride, ns = (size_t)std::max(mb->nsnap, 1);
-    TRY(e->get(("stage0" + tag).c_str(), fs, &mb->stage[0]));
-    TRY(e->get(("stage1" + tag).c_str(), fs, &mb->stage[1]));
+    for (int i = 0; i < 4; ++i) TRY(e->get(("stage" + std::to_string(i) + tag).c_str(), fs, &mb->stage[i]));
     TRY(e->get(("amax" + tag).c_str(), ns, &mb->amax));
     TRY(e->get(("snap16" + tag).c_str(), ns * fs, &mb->snap16));
     TRY(e->get(("iscale" + tag).c_str(), ns, &mb->iscale));
     TRY(e->get(("comp" + tag).c_str(), fs, &mb->comp));
     // The staging buffers' pad rows are converted too: keep them zero.
-    CUDA_TRY(cudaMemsetAsync(mb->stage[0], 0, fs * sizeof(float), e->stream));
-    CUDA_TRY(cudaMemsetAsync(mb->stage[1], 0, fs * sizeof(float), e->stream));
+    for (float* b : mb->stage) CUDA_TRY(cudaMemsetAsync(b, 0, fs * sizeof(float), e->stream));
     CUDA_TRY(cudaMemsetAsync(mb->amax, 0, ns * sizeof(unsigned int), e->stream));
     CUDA_TRY(cudaMemsetAsync(mb->comp, 0, fs * sizeof(float), e->stream));
     return PSDM_OK;
@@ -790,7 +1037,7 @@ void mixed_forward_args(const MixedBufs& mb, std::vector<StepArgs>& steps, size_
         a.field_amax = nullptr;
         a.q_src = nullptr;
         if (prev > 0) {
-            a.q_src = mb.stage[prev & 1];
+            a.q_src = mb.stage[prev & 3];
             a.q_amax = mb.amax + (prev - 1);
             a.q_dst = mb.snap16 + (size_t)(prev - 1) * mb.fstride;
             a.q_iscale = mb.iscale + (prev - 1);
@@ -800,7 +1047,7 @@ void mixed_forward_args(const MixedBufs& mb, std::vector<StepArgs>& steps, size_
         if ((k - 1) % mb.ks == 0) {
             const int m = (k - 1) / mb.ks;
             if (m >= 1 && m <= mb.nsnap) {
-                a.field = mb.stage[m & 1];
+                a.field = mb.stage[m & 3];
                 a.field_amax = mb.amax + (m - 1);
                 prev = m;
             }
@@ -811,7 +1058,7 @@ void mixed_forward_args(const MixedBufs& mb, std::vector<StepArgs>& steps, size_
 
 int mixed_quantize(psdm_engine* e, const MixedBufs& mb, int m) {
     if (m <= 0) return PSDM_OK;
-    const int rc = launch_quantize(mb.stage[m & 1], mb.amax + (m - 1), mb.snap16 + (size_t)(m - 1) * mb.fstride,
+    const int rc = launch_quantize(mb.stage[m & 3], mb.amax + (m - 1), mb.snap16 + (size_t)(m - 1) * mb.fstride,
                                    mb.iscale + (m - 1), (int)mb.fstride, mb.kind, e->stream);
     if (rc) return fail(PSDM_ERR_CUDA, "snapshot conversion launch: %s", cudaGetErrorString((cudaError_t)rc));
     e->launches += 1;
@@ -1001,21 +1248,40 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
         TRY(mixed_bufs(e, s, prm->precision, store_snap, nt_prop2, "", &mb));
         TRY(e->record(0));
         std::vector<StepArgs> fw;
-        TRY(build_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, "", &fw));
+        std::vector<int> row_slot;
+        TRY(build_forward(e, s, nt_prop2, store_snap, d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, "", &fw,
+                          false, &row_slot));
         int pending = 0;
         mixed_forward_args(mb, fw, 0, &pending);
-        TRY(launch_steps(e, 0, fw));
+        if (pair_on(e)) {
+            std::vector<PairArgs> pairs;
+            std::vector<int> pend;
+            float* last = nullptr;
+            TRY(make_pairs(e, s, 0, fw, 0, fw.size(), row_slot, 0, nullptr, &mb, "", &pairs, &last, &pend));
+            TRY(launch_pairs(e, 0, pairs));
+            for (int m : pend) TRY(mixed_quantize(e, mb, m));
+        } else {
+            TRY(launch_steps(e, 0, fw));
+            TRY(mixed_quantize(e, mb, pending));
+        }
         e->fwd_steps += nt_prop2 - 1;
-        TRY(mixed_quantize(e, mb, pending));
         TRY(e->record(1));
         const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, taper_option, N_taper, N_zeros);
         CUDA_TRY(cudaMemsetAsync(d_imgp, 0, fstride * sizeof(float), e->stream));
         TRY(reset_state(e, &s));
         std::vector<StepArgs> bw;
+        std::vector<int> brow;
         TRY(build_backward(e, s, nt_taper, store_snap, nt_taper, d_tgt, 1, NumRec, w.zr.data(), w.xr.data(), nullptr,
-                           1, 0, nullptr, d_imgp, "", &bw));
+                           1, 0, nullptr, d_imgp, "", &bw, nullptr, false, &brow));
         mixed_backward_args(mb, nt_taper, wts.data(), bw, 0);
-        TRY(launch_steps(e, 2, bw));
+        if (pair_on(e)) {
+            std::vector<PairArgs> pairs;
+            float* last = nullptr;
+            TRY(make_pairs(e, s, 2, bw, 0, bw.size(), brow, 0, nullptr, nullptr, "", &pairs, &last, nullptr));
+            TRY(launch_pairs(e, 2, pairs));
+        } else {
+            TRY(launch_steps(e, 2, bw));
+        }
         e->bwd_steps += nt_taper - 1;
         TRY(e->record(2));
         CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
@@ -1075,6 +1341,12 @@ struct BatchSlot {
     std::string tag;
     Shot s;
     StepArgs* d_args = nullptr;  // nfwd forward steps, then nbwd backward steps
+    // Pair launches (two steps each): nfwd forward launches, then nbwd
+    // backward launches; steps of each pass.
+    bool pairs = false;
+    PairArgs* d_pargs = nullptr;
+    int fwd_steps = 0, bwd_steps = 0;
+    std::vector<int> pend;         // mixed form, pair launches: slots staged by the last forward launch
     float* d_imgp = nullptr;     // pitched window image
     float* d_out = nullptr;      // device variant: caller's image
     float* h_out = nullptr;      // host variant: caller's image, pending copy-out
@@ -1146,24 +1418,48 @@ int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
     TRY(e->get(("imgp" + tag).c_str(), fstride, &sl.d_imgp));
     const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, j.taper_option, j.N_taper, j.N_zeros);
     std::vector<StepArgs> steps;
+    std::vector<int> frow, brow;
     TRY(build_forward(e, sl.s, nt_prop2, j.store_snap, j.d_S, w.zs, w.xs, d_F, nsnap, 0, nullptr, nullptr, tag,
-                      &steps, true));
+                      &steps, true, &frow));
     sl.nfwd = (int)steps.size();
     sl.pending = 0;
     if (mixed) mixed_forward_args(sl.mb, steps, 0, &sl.pending);
     TRY(build_backward(e, sl.s, nt_taper, j.store_snap, nt_taper, d_tgt, 1, sh.NumRec, w.zr.data(), w.xr.data(),
-                       d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps, nullptr, true));
+                       d_F, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps, nullptr, true, &brow));
     if (mixed) mixed_backward_args(sl.mb, nt_taper, wts.data(), steps, (size_t)sl.nfwd);
     sl.bwd_mode = mixed ? 2 : 1;
     sl.nbwd = (int)steps.size() - sl.nfwd;
-    sl.tiles[0] = sl.nfwd > 0 ? steps[0].r_first[steps[0].nrect] : 0;
-    sl.tiles[1] = sl.nbwd > 0 ? steps[sl.nfwd].r_first[steps[sl.nfwd].nrect] : 0;
-    const size_t abytes = steps.size() * sizeof(StepArgs);
-    StepArgs* h_args = nullptr;
-    TRY(e->get_pinned(("hargs" + tag).c_str(), abytes, (void**)&h_args));
-    std::memcpy(h_args, steps.data(), abytes);
-    TRY(e->get(("args" + tag).c_str(), abytes, (void**)&sl.d_args));
-    CUDA_TRY(cudaMemcpyAsync(sl.d_args, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
+    sl.fwd_steps = sl.nfwd;
+    sl.bwd_steps = sl.nbwd;
+    sl.pairs = pair_on(e);
+    if (sl.pairs) {
+        std::vector<PairArgs> pl;
+        float* last = nullptr;
+        TRY(make_pairs(e, sl.s, 0, steps, 0, (size_t)sl.nfwd, frow, 0, nullptr, mixed ? &sl.mb : nullptr, tag, &pl,
+                       &last, &sl.pend));
+        const int nf = (int)pl.size();
+        TRY(make_pairs(e, sl.s, sl.bwd_mode, steps, (size_t)sl.nfwd, (size_t)sl.nbwd, brow, 0, nullptr, nullptr, tag,
+                       &pl, &last, nullptr));
+        sl.nfwd = nf;
+        sl.nbwd = (int)pl.size() - nf;
+        sl.tiles[0] = sl.nfwd > 0 ? pl[0].r_first[pl[0].nrect] : 0;
+        sl.tiles[1] = sl.nbwd > 0 ? pl[nf].r_first[pl[nf].nrect] : 0;
+        const size_t abytes = pl.size() * sizeof(PairArgs);
+        PairArgs* h_args = nullptr;
+        TRY(e->get_pinned(("hargs" + tag).c_str(), abytes, (void**)&h_args));
+        std::memcpy(h_args, pl.data(), abytes);
+        TRY(e->get(("pargs" + tag).c_str(), abytes, (void**)&sl.d_pargs));
+        CUDA_TRY(cudaMemcpyAsync(sl.d_pargs, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
+    } else {
+        sl.tiles[0] = sl.nfwd > 0 ? steps[0].r_first[steps[0].nrect] : 0;
+        sl.tiles[1] = sl.nbwd > 0 ? steps[sl.nfwd].r_first[steps[sl.nfwd].nrect] : 0;
+        const size_t abytes = steps.size() * sizeof(StepArgs);
+        StepArgs* h_args = nullptr;
+        TRY(e->get_pinned(("hargs" + tag).c_str(), abytes, (void**)&h_args));
+        std::memcpy(h_args, steps.data(), abytes);
+        TRY(e->get(("args" + tag).c_str(), abytes, (void**)&sl.d_args));
+        CUDA_TRY(cudaMemcpyAsync(sl.d_args, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
+    }
     CUDA_TRY(cudaEventRecord(sl.staged, e->stream));
     CUDA_TRY(cudaMemsetAsync(sl.d_imgp, 0, fstride * sizeof(float), e->stream));
     sl.shot = i;
@@ -1218,9 +1514,9 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         const size_t nsnap = (size_t)(j.shots[i].nt_prop2 - 1) / j.store_snap;
         const size_t steps = (size_t)j.shots[i].nt_prop2 + j.shots[i].nt_taper;
         const size_t snap_bytes = j.prm->precision != PSDM_PREC_FP32
-                                      ? (nsnap * 2 + 4 * 4) * g.field_cells()   // 16-bit slots, 2 stages, comp, image
+                                      ? (nsnap * 2 + 6 * 4) * g.field_cells()   // 16-bit slots, 4 stages, comp, image
                                       : (nsnap + 1) * g.field_cells() * sizeof(float);
-        size_t b = 9 * g.cells() * sizeof(float) + snap_bytes + steps * sizeof(StepArgs);
+        size_t b = 13 * g.cells() * sizeof(float) + snap_bytes + steps * sizeof(PairArgs);
         if (j.host_io) b += ((size_t)j.ny * j.shots[i].nx_w + (size_t)j.shots[i].NumRec * j.shots[i].nt_taper) *
                             sizeof(float);
         per_slot = std::max(per_slot, b);
@@ -1267,21 +1563,31 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
     int sel = 0;
     while (rc == PSDM_OK) {
         BatchParams bp;
+        PairBatchParams pb;
         std::memset(&bp, 0, sizeof(bp));
+        std::memset(&pb, 0, sizeof(pb));
         int n = 0;
+        bool pairs = false;
         for (BatchSlot& sl : slots) {
             if (sl.shot < 0) continue;
-            bp.mode[n] = sl.pass == 0 ? 0 : sl.bwd_mode;
-            bp.args[n] = sl.d_args + (sl.pass == 0 ? sl.k : sl.nfwd + sl.k);
-            bp.first[n + 1] = bp.first[n] + sl.tiles[sl.pass];
+            pairs = sl.pairs;  // the same for every slot of a call
+            const int md = sl.pass == 0 ? 0 : sl.bwd_mode;
+            const int at = sl.pass == 0 ? sl.k : sl.nfwd + sl.k;
+            bp.mode[n] = pb.mode[n] = md;
+            if (sl.pairs)
+                pb.args[n] = sl.d_pargs + at;
+            else
+                bp.args[n] = sl.d_args + at;
+            bp.first[n + 1] = pb.first[n + 1] = bp.first[n] + sl.tiles[sl.pass];
             ++n;
         }
         if (n == 0) break;
-        bp.nslots = n;
-        bp.counter = counters;
-        bp.counter_sel = sel;
+        bp.nslots = pb.nslots = n;
+        bp.counter = pb.counter = counters;
+        bp.counter_sel = pb.counter_sel = sel;
         sel ^= 1;
-        const int lr = launch_batch_step(bp, e->num_sms, e->stream);
+        const int lr = pairs ? launch_pair_batch(pb, e->num_sms, e->stream)
+                             : launch_batch_step(bp, e->num_sms, e->stream);
         if (lr) {
             rc = fail(PSDM_ERR_CUDA, "batched step launch: %s", cudaGetErrorString((cudaError_t)lr));
             break;
@@ -1291,18 +1597,23 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
             if (sl.shot < 0) continue;
             sl.k += 1;
             if (sl.pass == 0) {
-                e->fwd_steps += 1;
                 if (sl.k < sl.nfwd) continue;
+                e->fwd_steps += sl.fwd_steps;
                 // Second propagator call on the same model: fresh wavefield.
-                if (sl.bwd_mode == 2) rc = mixed_quantize(e, sl.mb, sl.pending);
+                if (sl.bwd_mode == 2) {
+                    if (sl.pairs)
+                        for (int m : sl.pend) rc = rc == PSDM_OK ? mixed_quantize(e, sl.mb, m) : rc;
+                    else
+                        rc = mixed_quantize(e, sl.mb, sl.pending);
+                }
                 if (rc == PSDM_OK) rc = reset_state(e, &sl.s);
                 sl.pass = 1;
                 sl.k = 0;
                 if (rc != PSDM_OK) break;
                 if (sl.nbwd > 0) continue;
             } else {
-                e->bwd_steps += 1;
                 if (sl.k < sl.nbwd) continue;
+                e->bwd_steps += sl.bwd_steps;
             }
             rc = batch_finish(e, j, sl);
             sl.shot = -1;
@@ -1340,7 +1651,8 @@ int psdm_engine_create(int32_t device, psdm_engine** out) {
     if (device < 0 || device >= n) return fail(PSDM_ERR_ARG, "device %d out of range (%d devices)", device, n);
     CUDA_TRY(cudaSetDevice(device));
     {
-        const int rc = prepare_step_kernels();
+        int rc = prepare_step_kernels();
+        if (rc == 0) rc = prepare_pair_kernels();
         if (rc) return fail(PSDM_ERR_CUDA, "preparing the step kernels: %s", cudaGetErrorString((cudaError_t)rc));
     }
     psdm_engine* e = new psdm_engine();
@@ -1602,6 +1914,14 @@ int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slot
 int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on) {
     TRY(check_engine(e));
     e->use_pass = on != 0;
+    return PSDM_OK;
+}
+
+int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps) {
+    TRY(check_engine(e));
+    if (steps != 1 && steps != 2) return fail(PSDM_ERR_ARG, "steps per launch must be 1 or 2 (got %d)", steps);
+    TRY(sync(e));
+    e->steps_per_launch = steps;
     return PSDM_OK;
 }
 

@@ -154,6 +154,88 @@ struct BatchParams {
     const StepArgs* args[kMaxSlots];
 };
 
+// ---- Two time steps per launch (rtm_pair.cu) ------------------------------
+//
+// A pair launch advances the grid from levels (n-1, n) to (n+1, n+2): each
+// tile loads level n on itself plus a 6-cell ring, computes level n+1 on
+// itself plus a 3-cell ring in shared memory (the ring is recomputed,
+// bit-identically, by the neighbouring tiles), then level n+2 on itself.
+// Inputs are only read and outputs go to other buffers, so the wavefield
+// rotates through four buffers, the C-PML variables through two each and
+// the free-surface histories through four.
+
+// Per-step values of one sub-step of a pair launch.
+struct SubStep {
+    float* field;               // forward: snapshot written (FP32, or the mixed form's staging buffer);
+                                // backward: FP32 snapshot read; null = none at this sub-step
+    const void* field16;        // mixed backward: 16-bit snapshot read, or null
+    const float* field_iscale;  // its inverse scale 2^-k
+    unsigned int* field_amax;   // mixed forward: largest |snapshot| (float bits), or null
+    float field_w;              // taper weight of the snapshot slot
+    int inj_t;                  // injection sample index of this step
+    int rec_t;                  // forward: receiver sample taken from this sub-step's level, or -1
+    int pad_;
+};
+
+constexpr int kPairRects = 48;
+
+struct PairArgs {
+    // Common fields.  a.p = level n (read on tile + 6), a.pm = level n-1
+    // (read on tile + 3), a.phix_in / a.phiz_in = phi at level n, a.phix_out
+    // / a.phiz_out = phi at level n + nsub, a.chix / a.chiz = chi at level
+    // n + nsub (written), a.side_p / a.side_pm = free-surface histories at
+    // levels n / n-1, a.q_* = the first snapshot conversion of the launch's
+    // prologue.  a's per-step fields and tile plan are not used.
+    StepArgs a;
+    const float* chix_in;  // chi at level n
+    const float* chiz_in;
+    float* p_out[2];       // levels n+1, n+2
+    float* side_out[2];    // free-surface histories at levels n+1, n+2
+    SubStep sub[2];
+    int nsub;              // 2: two steps; 1: one step (outputs at level n+1 only)
+    int txc;               // columns of the clean interior tiles the plan was made for
+    // second conversion of the prologue (two snapshots per launch)
+    int q_n2;
+    const float* q_src2;
+    const unsigned int* q_amax2;
+    void* q_dst2;
+    float* q_iscale2;
+    // receivers whose cell lies in tile b: rec_idx[rec_first[b] .. rec_first[b+1])
+    const int* rec_first;
+    const int* rec_idx;
+    // Tile plan: rect r of type r_type (0 clean interior, 1 generic) covers
+    // device rows [r_zd0, r_zd0 + r_h) x columns [r_x0, r_x0 + r_w), split
+    // into r_tz x r_tx tiles, blocks [r_first[r], r_first[r+1]).
+    int nrect;
+    int r_type[kPairRects], r_zd0[kPairRects], r_x0[kPairRects], r_h[kPairRects], r_w[kPairRects];
+    int r_tz[kPairRects], r_tx[kPairRects], r_first[kPairRects + 1];
+};
+
+// Plan the tiles of a pair launch from P->a's grid fields and the host copy
+// of the injection row map (ldz entries or null).  Returns false if the plan
+// needs more than kPairRects rectangles.
+bool plan_pair(PairArgs* P, const int* row_slot_host);
+// Cell rectangle [z0, z1) x [x0, x1) (device rows, columns) of tile b.
+void pair_tile_rect(const PairArgs& P, int b, int* z0, int* z1, int* x0, int* x1);
+// Receivers (linear cells x * ldz + device row) held by each tile, as offsets.
+void pair_rec_lists(const PairArgs& P, int nrec, const int* h_rec_cell, std::vector<int>* first,
+                    std::vector<int>* idx);
+int prepare_pair_kernels();
+// One pair launch of pass `mode` (0 forward, 1 backward, 2 mixed backward).
+int launch_pair(int mode, const PairArgs& P, void* stream);
+
+// Several shots per pair launch: slot s runs pass mode[s] with the arguments
+// at args[s] (device memory), tiles [first[s], first[s+1]).
+struct PairBatchParams {
+    int nslots;
+    int counter_sel;
+    int* counter;
+    int mode[kMaxSlots];
+    int first[kMaxSlots + 1];
+    const PairArgs* args[kMaxSlots];
+};
+int launch_pair_batch(const PairBatchParams& bp, int num_sms, void* stream);
+
 // Fill the block decomposition of `a` from its grid fields (nyt, nxt, ny,
 // nx, dn, zoff, fs) and the host copy of the injection row map (ldz
 // entries, or null when nothing is injected).  `batched` plans the interior

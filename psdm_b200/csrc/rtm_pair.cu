@@ -1,0 +1,901 @@
+// Two time steps per launch (temporal blocking) for sm_100a.
+//
+// The same per-cell arithmetic as the one-step kernels (rtm_step.cu), which
+// follow src/solver_ac_forward_ram.f90:344-573 and
+// src/solver_ac_backward_ram.f90:329-545 in the reference's evaluation
+// order, organised so that a launch advances the grid by two steps:
+//
+//   * a tile loads level n on itself plus a 6-cell ring, computes level n+1
+//     on itself plus a 3-cell ring into shared memory (the ring cells are
+//     computed again, with the same arithmetic, by the tiles that own them),
+//     and then level n+2 on itself;
+//   * levels n-1 and n are only read, levels n+1 and n+2 go to two other
+//     buffers (the wavefield rotates through four); the C-PML memory
+//     variables phi and chi read level n and write level n+2 to a second
+//     buffer, level n+1 living only in shared memory; the free-surface
+//     histories rotate like the wavefield;
+//   * both steps' snapshots (forward) or imaging updates (backward), source
+//     or adjoint-source injections and receiver samples are done by the tile
+//     that owns the cell, in step order.
+//
+// Per step and cell the wavefield crosses HBM half as often as with one
+// launch per step (p, p1 and c2 are read once for two steps) and the launch
+// count halves.  A launch may also do a single step (nsub = 1), which ends a
+// pass with an odd number of steps.
+//
+// Tiles: "clean" interior tiles (rect type 0) whose tile and 3-cell ring
+// hold only interior cells with no injection and no free-surface row, 120
+// rows x 28 columns, level n staged in shared memory by bulk asynchronous
+// copies, each thread sliding a float4 x 7-column window through registers
+// with the packed FP32x2 stencil of the one-step interior tiles; and
+// "generic" tiles (rect type 1, at most 32 x 32 cells) for everything else:
+// C-PML strips and corners (with the phi/chi recursions of
+// src/solver_PML_matrices.f90:1-111), the free-surface and injection rows,
+// and the interior cells next to them, one cell per thread at a time.
+//
+// Reach: a cell's update reads its neighbours within 3 cells, except where
+// a stencil centre is clamped (the reference copies the derivative at
+// acc+1 into the first acc cells, src/solver_space_derivs_clean.f90) or a
+// strip-local phi derivative is clamped to its strip
+// (src/solver_PML_matrices.f90:9-38); those reads reach up to 6 cells, but
+// always towards the inside of the grid or strip.  The planner therefore
+// starts tiles at every strip and grid edge and keeps them at least 8 cells
+// wide and high there, so that every read of level n+1 by a tile's cells
+// lies in its 3-cell ring and every read of level n by the ring lies within
+// 6 cells.
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "rtm_device.cuh"
+#include "rtm_internal.h"
+
+namespace psdm {
+namespace {
+
+// Clean interior tiles: TZC output rows (30 float4 rows; level n+1 is
+// computed on 32 float4 rows, one per lane) by TXC columns.
+constexpr int TZC = 120;
+constexpr int XSC = 7;              // output columns per warp
+constexpr int TXC = NWARP * XSC;    // 28
+constexpr int HS0 = TZC + 16;       // rows of the level-n tile (6-row ring rounded up to 8)
+constexpr int HS1 = TZC + 8;        // rows of the level n+1 tile (3-row ring rounded up to 4)
+constexpr int Q0 = HS0 / 4, Q1 = HS1 / 4;
+constexpr int WS0 = TXC + 12, WS1 = TXC + 6;
+constexpr int kCleanFloats = HS0 * WS0 + HS1 * WS1;
+// Generic tiles: at most GZ x GX cells.
+constexpr int GZ = 32, GX = 32;
+constexpr int GH0 = GZ + 12, GW0 = GX + 12;  // level n on the tile + 6
+constexpr int GH1 = GZ + 6, GW1 = GX + 6;    // level n+1, phi and chi at n+1 on the tile + 3
+constexpr int kGenericFloats = GH0 * GW0 + 5 * GH1 * GW1 + GW1;
+constexpr int kPairFloats = kCleanFloats > kGenericFloats ? kCleanFloats : kGenericFloats;
+
+// Largest |snapshot| of each sub-step seen by this block (float bits).
+__shared__ unsigned int s_pair_amax[2];
+
+// The packed FP32x2 interior update of the one-step interior tiles for one
+// float4 of rows: win = the 7 x-neighbour columns (centre win[3]), zm / zp =
+// the float4s above and below the centre, pmv = level n-1 of the float4,
+// c2v = its c2.  Tap sums and products are packed; every add that consumes
+// a fresh product is scalar, so no multiply-add is ever fused.
+__device__ __forceinline__ float4 clean_update(const float4 (&win)[7], const float4& zm, const float4& zp,
+                                               const float4& pmv, const float4& c2v, const float2 (&cc)[4]) {
+    const float4& pc = win[3];
+    const float2 z01 = make_float2(zm.y, zm.z), z12 = make_float2(zm.z, zm.w);
+    const float2 z23 = make_float2(zm.w, pc.x), z34 = lo2(pc);
+    const float2 z45 = make_float2(pc.y, pc.z), z56 = hi2(pc);
+    const float2 z67 = make_float2(pc.w, zp.x), z78 = lo2(zp);
+    const float2 z89 = make_float2(zp.y, zp.z);
+#define XA(k) lo2(win[3 + (k)])
+#define XB(k) hi2(win[3 + (k)])
+    const float2 d2xA = D2P(XA, cc);
+    const float2 d2xB = D2P(XB, cc);
+#undef XA
+#undef XB
+    const float2 zA[7] = {z01, z12, z23, z34, z45, z56, z67};
+    const float2 zB[7] = {z23, z34, z45, z56, z67, z78, z89};
+#define ZA(k) zA[3 + (k)]
+#define ZB(k) zB[3 + (k)]
+    const float2 d2yA = D2P(ZA, cc);
+    const float2 d2yB = D2P(ZB, cc);
+#undef ZA
+#undef ZB
+    // -p1 + 2p: 2p is exact, so a fused form would round identically
+    const float2 two = make_float2(2.f, 2.f);
+    const float2 baseA = __fadd2_rn(neg2(lo2(pmv)), __fmul2_rn(two, lo2(pc)));
+    const float2 baseB = __fadd2_rn(neg2(hi2(pmv)), __fmul2_rn(two, hi2(pc)));
+    const float2 oA = add_prod(baseA, __fmul2_rn(lo2(c2v), __fadd2_rn(d2xA, d2yA)));
+    const float2 oB = add_prod(baseB, __fmul2_rn(hi2(c2v), __fadd2_rn(d2xB, d2yB)));
+    return make_float4(oA.x, oA.y, oB.x, oB.y);
+}
+
+// Snapshot (forward) or imaging update (backward) of one float4 of interior
+// cells at offset fi of the pitched snapshot / image: out = the new level,
+// pmv = the level two steps back.  Fc / Ic / Cc / Frc: prefetched snapshot,
+// image, compensation and raw 16-bit snapshot values.
+template <int MODE>
+__device__ __forceinline__ void emit4(const StepArgs& a, const SubStep& s, int fi, const float4& out,
+                                      const float4& pmv, float4 Fc, const float4& Ic, const float4& Cc,
+                                      const uint2& Frc, float isc, float& amax_t) {
+    if (MODE == 0) {
+        const float hx = __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f);
+        const float hy = __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f);
+        const float hz = __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f);
+        const float hw = __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f);
+        bool rare = false;
+        float4 sv;
+        sv.x = div_dt_common(a, hx, rare);
+        sv.y = div_dt_common(a, hy, rare);
+        sv.z = div_dt_common(a, hz, rare);
+        sv.w = div_dt_common(a, hw, rare);
+        if (__any_sync(__activemask(), rare) && rare) {
+            sv.x = div_dt(a, hx);
+            sv.y = div_dt(a, hy);
+            sv.z = div_dt(a, hz);
+            sv.w = div_dt(a, hw);
+        }
+        *reinterpret_cast<float4*>(s.field + fi) = sv;
+        if (s.field_amax != nullptr)
+            amax_t = fmaxf(amax_t, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(sv.z), fabsf(sv.w))));
+    } else if (MODE == 1) {
+        if (s.field_w != 1.f) {
+            Fc.x = __fmul_rn(Fc.x, s.field_w); Fc.y = __fmul_rn(Fc.y, s.field_w);
+            Fc.z = __fmul_rn(Fc.z, s.field_w); Fc.w = __fmul_rn(Fc.w, s.field_w);
+        }
+        const float2 half = make_float2(0.5f, 0.5f);
+        const float2 oA = lo2(out), oB = hi2(out);
+        float2 iA = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oA, neg2(lo2(pmv)))), lo2(Fc));
+        float2 iB = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oB, neg2(hi2(pmv)))), hi2(Fc));
+        if (a.ss != 1.f) {
+            const float2 ss = make_float2(a.ss, a.ss);
+            iA = __fmul2_rn(iA, ss);
+            iB = __fmul2_rn(iB, ss);
+        }
+        const float2 rA = add_prod(lo2(Ic), iA), rB = add_prod(hi2(Ic), iB);
+        *reinterpret_cast<float4*>(a.image + fi) = make_float4(rA.x, rA.y, rB.x, rB.y);
+    } else {
+        const float4 F4 = unpack16x4(Frc, a.kind16, isc);
+        float Fv[4] = {F4.x, F4.y, F4.z, F4.w};
+        float Iv[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
+        float Cv[4] = {Cc.x, Cc.y, Cc.z, Cc.w};
+        const float ov[4] = {out.x, out.y, out.z, out.w};
+        const float pv[4] = {pmv.x, pmv.y, pmv.z, pmv.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float F = Fv[e];
+            if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
+            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(ov[e], pv[e])), F);
+            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+            kahan(Iv[e], Cv[e], inc);
+        }
+        *reinterpret_cast<float4*>(a.image + fi) = make_float4(Iv[0], Iv[1], Iv[2], Iv[3]);
+        *reinterpret_cast<float4*>(a.comp + fi) = make_float4(Cv[0], Cv[1], Cv[2], Cv[3]);
+    }
+}
+
+// One phase of a clean interior tile (rows [z0, z0+nrows), a multiple of 4
+// starting on a float4 boundary; columns [x0, x0+ncols)).
+//   PH = 0: level n+1 on rows [z0-4, z0+nrows+4) x columns [x0-3,
+//     x0+ncols+3) from level n in S0 (rows from z0-8, columns from x0-6) and
+//     level n-1 from HBM, into S1 (rows from z0-4, columns from x0-3); on the
+//     tile also to p_out[0], with sub-step 0's snapshot or imaging.
+//   PH = 1: level n+2 on the tile from S1, with level n from S0, to p_out[1]
+//     and over level n in S0 (for the receiver gather), with sub-step 1's
+//     snapshot or imaging.
+// Lane l owns the float4 of rows z0-4+4l (PH 0) or z0+4l (PH 1); warp w a
+// run of consecutive columns, swept with a 7-column register window.
+template <int MODE, int PH>
+__device__ __forceinline__ void clean_phase(const PairArgs& P, float* S0, float* S1, int z0, int x0, int nrows,
+                                            int ncols, const float2 (&cc)[4]) {
+    const StepArgs& a = P.a;
+    const SubStep& s = P.sub[PH];
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int nq = PH == 0 ? (nrows >> 2) + 2 : (nrows >> 2);
+    const int ncl = PH == 0 ? ncols + 6 : ncols;
+    const int cb = (w * ncl) >> 2, ce = ((w + 1) * ncl) >> 2;
+    if (lane >= nq || cb >= ce) return;
+    const int zd = PH == 0 ? z0 - 4 + 4 * lane : z0 + 4 * lane;
+    constexpr int SQ = PH == 0 ? Q0 : Q1;
+    const float4* __restrict__ src = reinterpret_cast<const float4*>(PH == 0 ? S0 : S1);
+    float4* S0v = reinterpret_cast<float4*>(S0);
+    float4* S1v = reinterpret_cast<float4*>(S1);
+    const int sr = lane + 1;  // float4 row of this thread's float4 in the source tile
+    const bool rowT = PH == 1 || (lane >= 1 && lane <= (nrows >> 2));
+    const int xb = PH == 0 ? x0 - 3 : x0;  // column of phase column 0
+    const int tc0 = PH == 0 ? 3 : 0, tc1 = PH == 0 ? ncols + 3 : ncols;
+    const int dn = a.dn;
+    const bool snap = MODE == 0 && s.field != nullptr;
+    const bool img = MODE == 1 && s.field != nullptr;
+    const bool img16 = MODE == 2 && s.field16 != nullptr;
+    const float isc = img16 ? __ldg(s.field_iscale) : 1.f;
+    float amax_t = 0.f;
+    int g = (xb + cb) * a.ldz + zd;
+    int fi = (xb + cb - dn) * a.ldf + (zd - a.zoff - dn);
+    float4 pmN = PH == 0 ? *reinterpret_cast<const float4*>(a.pm + g) : S0v[(cb + 6) * Q0 + lane + 2];
+    float4 c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
+    float4 Fn = make_float4(0.f, 0.f, 0.f, 0.f), In = Fn, Cn = Fn;
+    uint2 Fr = make_uint2(0u, 0u);
+    if (rowT && cb >= tc0 && cb < tc1) {
+        if (img) {
+            Fn = __ldg(reinterpret_cast<const float4*>(s.field + fi));
+            In = *reinterpret_cast<const float4*>(a.image + fi);
+        }
+        if (img16) {
+            Fr = load16x4_raw(s.field16, fi);
+            In = *reinterpret_cast<const float4*>(a.image + fi);
+            Cn = *reinterpret_cast<const float4*>(a.comp + fi);
+        }
+    }
+    float4 win[7];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) win[k] = src[(cb + k) * SQ + sr];
+#pragma unroll 1
+    for (int c = cb; c < ce; ++c) {
+        win[6] = src[(c + 6) * SQ + sr];
+        const float4 zm = src[(c + 3) * SQ + sr - 1];
+        const float4 zp = src[(c + 3) * SQ + sr + 1];
+        const float4 pmv = pmN, c2v = c2N;
+        if (c + 1 < ce) {
+            pmN = PH == 0 ? *reinterpret_cast<const float4*>(a.pm + g + a.ldz) : S0v[(c + 7) * Q0 + lane + 2];
+            c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g + a.ldz));
+        }
+        const float4 Fc = Fn, Ic = In, Cc = Cn;
+        const uint2 Frc = Fr;
+        const bool t = rowT && c >= tc0 && c < tc1;
+        if (c + 1 < ce && rowT && c + 1 >= tc0 && c + 1 < tc1) {
+            if (img) {
+                Fn = __ldg(reinterpret_cast<const float4*>(s.field + fi + a.ldf));
+                In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
+            }
+            if (img16) {
+                Fr = load16x4_raw(s.field16, fi + a.ldf);
+                In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
+                Cn = *reinterpret_cast<const float4*>(a.comp + fi + a.ldf);
+            }
+        }
+        const float4 out = clean_update(win, zm, zp, pmv, c2v, cc);
+        if (PH == 0) S1v[c * Q1 + lane] = out;
+        if (t) {
+            *reinterpret_cast<float4*>(P.p_out[PH] + g) = out;
+            if (PH == 1) S0v[(c + 6) * Q0 + lane + 2] = out;
+            if (snap || img || img16) emit4<MODE>(a, s, fi, out, pmv, Fc, Ic, Cc, Frc, isc, amax_t);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) win[k] = win[k + 1];
+        g += a.ldz;
+        fi += a.ldf;
+    }
+    if (snap && s.field_amax != nullptr && amax_t > 0.f) atomicMax(&s_pair_amax[PH], __float_as_uint(amax_t));
+}
+
+// Receiver samples of tile b (forward): sub-step 0's level from S1, sub-step
+// 1's from S0.  (oz0, ox0) / (oz1, ox1) are the origins (device row, column)
+// of S0 / S1, with pitches h0 / h1.
+__device__ __forceinline__ void gather_receivers(const PairArgs& P, int b, const float* S0, int oz0, int ox0, int h0,
+                                                 const float* S1, int oz1, int ox1, int h1) {
+    const StepArgs& a = P.a;
+    const int j0 = P.rec_first[b], j1 = P.rec_first[b + 1];
+    if (j1 <= j0) return;
+    __syncthreads();  // both levels complete
+    const int t0 = P.sub[0].rec_t, t1 = P.nsub == 2 ? P.sub[1].rec_t : -1;
+    for (int j = j0 + threadIdx.y * 32 + threadIdx.x; j < j1; j += NT) {
+        const int i = P.rec_idx[j];
+        const int cell = a.rec_cell[i];
+        const int x = cell / a.ldz, zd = cell - x * a.ldz;
+        if (t0 >= 0) a.rec_out[(size_t)i * a.rec_ld + t0] = S1[(x - ox1) * h1 + (zd - oz1)];
+        if (t1 >= 0) a.rec_out[(size_t)i * a.rec_ld + t1] = S0[(x - ox0) * h0 + (zd - oz0)];
+    }
+}
+
+// Clean interior tile t of rect r (tile b of the launch).  Returns false if
+// its bulk copies did not complete (error reported).
+template <int MODE>
+__device__ __forceinline__ bool pair_clean_tile(const PairArgs& P, float* sm, uint64_t* bar, uint32_t& phase, int r,
+                                                int t, int b) {
+    const StepArgs& a = P.a;
+    const int lane = threadIdx.x, wy = threadIdx.y;
+    if (P.txc != TXC) {  // planned for another tile width: report, touch nothing
+        if (lane == 0 && wy == 0) atomicExch(a.err, 2);
+        return false;
+    }
+    const int tz = t % P.r_tz[r], tx = t / P.r_tz[r];
+    const int z0 = P.r_zd0[r] + tz * TZC, x0 = P.r_x0[r] + tx * TXC;
+    const int nrows = min(TZC, P.r_zd0[r] + P.r_h[r] - z0);  // a multiple of 4
+    const int ncols = min(TXC, P.r_x0[r] + P.r_w[r] - x0);
+    float* S0 = sm;
+    float* S1 = sm + HS0 * WS0;
+    if (wy == 0) {  // level n, rows [z0-8, z0+nrows+8) x columns [x0-6, x0+ncols+6)
+        const uint32_t prow = (uint32_t)(nrows + 16) * 4u;
+        const uint32_t bytes = (uint32_t)(ncols + 12) * prow;
+        fence_proxy_async();  // the previous tile's shared accesses precede these writes
+        if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+        __syncwarp();
+        for (int c = lane; c < ncols + 12; c += 32)
+            bulk_g2s(S0 + c * HS0, a.p + (size_t)(x0 - 6 + c) * a.ldz + (z0 - 8), prow, bar);
+    }
+    float2 cc[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cc[k] = make_float2(a.cf2[k], a.cf2[k]);
+    const bool ok = mbar_wait_bounded(bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+        if (lane == 0 && wy == 0) atomicExch(a.err, 1);
+        return false;
+    }
+    clean_phase<MODE, 0>(P, S0, S1, z0, x0, nrows, ncols, cc);
+    if (P.nsub == 2) {
+        __syncthreads();
+        clean_phase<MODE, 1>(P, S0, S1, z0, x0, nrows, ncols, cc);
+    }
+    if (MODE == 0 && P.rec_first != nullptr) gather_receivers(P, b, S0, z0 - 8, x0 - 6, HS0, S1, z0 - 4, x0 - 3, HS1);
+    return true;
+}
+
+// Shared-memory views of a generic tile (rows [z0, z1) x columns [x0, x1)).
+struct GenTile {
+    float* S0;   // level n on rows [z0-6, z1+6) x columns [x0-6, x1+6), pitch GH0
+    float* S1;   // level n+1 on rows [z0-3, z1+3) x columns [x0-3, x1+3), pitch GH1
+    float* F1x;  // phi_x, phi_z, chi_x, chi_z at level n+1, laid out like S1
+    float* F1z;
+    float* X1x;
+    float* X1z;
+    float* SD1;  // free-surface history at level n+1 by column (from x0-3)
+    int z0, z1, x0, x1;
+};
+
+// One cell of a generic tile at sub-step SUB: the one-step kernels' generic
+// cell update (rtm_step.cu, cell_generic) with its sources moved:
+//   SUB 0: stencil level n from S0, level n-1 / phi / chi at level n and the
+//     free-surface histories (levels n, n-1) from HBM; results to S1 and the
+//     phi / chi / history tiles, and on the tile to the level n+1 outputs;
+//   SUB 1: stencil level n+1 from S1, level n from S0, phi / chi / history
+//     at level n+1 from shared memory and the history at level n from HBM;
+//     results to the level n+2 outputs (and over level n in S0).
+template <int MODE, int SUB>
+__device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, int zd, int x) {
+    const StepArgs& a = P.a;
+    const SubStep& s = P.sub[SUB];
+    const int dn = a.dn;
+    const int z = zd - a.zoff;
+    const int i1 = (x - (G.x0 - 3)) * GH1 + (zd - (G.z0 - 3));
+    const int i0 = (x - (G.x0 - 6)) * GH0 + (zd - (G.z0 - 6));
+    if (z < 0 || z >= a.nyt || x < 0 || x >= a.nxt || (a.fs && z < dn)) {
+        // outside the grid, or above a free surface: never updated, zero
+        if (SUB == 0) G.S1[i1] = 0.f;
+        return;
+    }
+    const bool inT = SUB == 1 || (zd >= G.z0 && zd < G.z1 && x >= G.x0 && x < G.x1);
+    const int kz = (z < dn) ? (dn - z) : (z >= dn + a.ny ? z - (dn + a.ny) + 1 : 0);
+    const int kx = (x < dn) ? (dn - x) : (x >= dn + a.nx ? x - (dn + a.nx) + 1 : 0);
+    const bool fsrow = a.fs && z == dn;
+    const bool side = fsrow && kx > 0 && !a.disk;
+    const float* SS = SUB == 0 ? G.S0 : G.S1;
+    constexpr int SP = SUB == 0 ? GH0 : GH1;
+    const int oz = SUB == 0 ? G.z0 - 6 : G.z0 - 3, ox = SUB == 0 ? G.x0 - 6 : G.x0 - 3;
+    const int cx = clampi(x, 3, a.nxt - 4);
+    const int czd = clampi(z, 3, a.nyt - 4) + a.zoff;
+    const float* colc = SS + (cx - ox) * SP + (zd - oz);  // x-stencil centre
+    const float* colz = SS + (x - ox) * SP + (czd - oz);  // z-stencil centre
+#define AX(k) colc[(k) * SP]
+#define AZ(k) colz[(k)]
+    const float d2x = D2(AX, a.cf2);
+    const float d2y = D2(AZ, a.cf2);
+    const int g = x * a.ldz + zd;
+    const float pc = SS[(x - ox) * SP + (zd - oz)];
+    const float pmo = SUB == 0 ? a.pm[g] : G.S0[i0];
+    const float c2v = __ldg(a.c2 + g);
+    float pp = pc, ppm = pmo;
+    if (side) {
+        if (SUB == 0) {
+            pp = a.side_p[x];
+            ppm = a.side_pm[x];
+        } else {
+            pp = G.SD1[x - (G.x0 - 3)];
+            ppm = a.side_p[x];
+        }
+    }
+    const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
+    float main_term, propz = 0.f;
+    if (kx > 0 || kz > 0) {
+        const int f = (kx > 0 && kz > 0) ? max(kx, kz) : (kx > 0 ? kx : kz);
+        const float A = __ldg(a.fA + f - 1), B = __ldg(a.fB + f - 1);
+        float propx = 0.f;
+        if (kx > 0) {
+            const float d1 = D1(AX, a.cf1);
+            const int sb = (x < dn) ? 0 : dn + a.nx;
+            const int ci = clampi(x - sb, 3, dn - 4) + sb;
+            float dph, phold, chold;
+            if (SUB == 0) {
+                const float* ph = a.phix_in + (size_t)ci * a.ldz + zd;
+#define PX(k) ph[(k) * a.ldz]
+                dph = D1(PX, a.cf1);
+#undef PX
+                phold = a.phix_in[g];
+                chold = P.chix_in[g];
+            } else {
+                const float* ph = G.F1x + (ci - (G.x0 - 3)) * GH1 + (zd - (G.z0 - 3));
+#define PX(k) ph[(k) * GH1]
+                dph = D1(PX, a.cf1);
+#undef PX
+                phold = G.F1x[i1];
+                chold = G.X1x[i1];
+            }
+            const float phn = __fadd_rn(__fmul_rn(A, phold), __fmul_rn(B, d1));
+            const float chn = __fadd_rn(__fmul_rn(A, chold), __fmul_rn(B, __fadd_rn(d2x, dph)));
+            if (SUB == 0) {
+                G.F1x[i1] = phn;
+                G.X1x[i1] = chn;
+                if (inT && P.nsub == 1) {
+                    a.phix_out[g] = phn;
+                    a.chix[g] = chn;
+                }
+            } else {
+                a.phix_out[g] = phn;
+                a.chix[g] = chn;
+            }
+            propx = __fadd_rn(dph, chn);
+        }
+        if (kz > 0) {
+            const float d1 = D1(AZ, a.cf1);
+            const int sb = (z < dn) ? 0 : dn + a.ny;
+            const int cj = clampi(z - sb, 3, dn - 4) + sb + a.zoff;
+            float dph, phold, chold;
+            if (SUB == 0) {
+                const float* ph = a.phiz_in + (size_t)x * a.ldz + cj;
+#define PZ(k) ph[(k)]
+                dph = D1(PZ, a.cf1);
+#undef PZ
+                phold = a.phiz_in[g];
+                chold = P.chiz_in[g];
+            } else {
+                const float* ph = G.F1z + (x - (G.x0 - 3)) * GH1 + (cj - (G.z0 - 3));
+#define PZ(k) ph[(k)]
+                dph = D1(PZ, a.cf1);
+#undef PZ
+                phold = G.F1z[i1];
+                chold = G.X1z[i1];
+            }
+            const float phn = __fadd_rn(__fmul_rn(A, phold), __fmul_rn(B, d1));
+            const float chn = __fadd_rn(__fmul_rn(A, chold), __fmul_rn(B, __fadd_rn(d2y, dph)));
+            if (SUB == 0) {
+                G.F1z[i1] = phn;
+                G.X1z[i1] = chn;
+                if (inT && P.nsub == 1) {
+                    a.phiz_out[g] = phn;
+                    a.chiz[g] = chn;
+                }
+            } else {
+                a.phiz_out[g] = phn;
+                a.chiz[g] = chn;
+            }
+            propz = __fadd_rn(dph, chn);
+        }
+        main_term = (kx > 0) ? propx : propz;
+    } else {
+        float src = 0.f;
+        if (a.row_slot != nullptr) {
+            const int rs = __ldg(a.row_slot + zd);
+            if (rs >= 0) {
+                const int j = __ldg(a.inj_cols + rs * a.nxt + x);
+                if (j >= 0) src = __ldg(a.inj_trace + (size_t)j * a.inj_ld + s.inj_t);
+            }
+        }
+        main_term = src;
+    }
+#undef AX
+#undef AZ
+    float p3 = __fadd_rn(base, __fmul_rn(c2v, __fadd_rn(__fadd_rn(d2x, d2y), main_term)));
+    if (kx > 0 && kz > 0) p3 = __fadd_rn(p3, __fmul_rn(c2v, propz));
+    float out = p3;
+    if (fsrow && (kx == 0 || !a.disk)) out = 0.f;
+    if (SUB == 0) {
+        G.S1[i1] = out;
+        if (side) G.SD1[x - (G.x0 - 3)] = p3;
+        if (inT) {
+            P.p_out[0][g] = out;
+            if (side) P.side_out[0][x] = p3;
+        }
+    } else {
+        P.p_out[1][g] = out;
+        G.S0[i0] = out;
+        if (side) P.side_out[1][x] = p3;
+    }
+    if (inT && kx == 0 && kz == 0) {
+        const int fi = (x - dn) * a.ldf + (z - dn);
+        if (MODE == 0) {
+            if (s.field != nullptr) {
+                const float D = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
+                s.field[fi] = D;
+                if (s.field_amax != nullptr) atomicMax(&s_pair_amax[SUB], __float_as_uint(fabsf(D)));
+            }
+        } else if (MODE == 1) {
+            if (s.field != nullptr) {
+                float F = __ldg(s.field + fi);
+                if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
+                float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
+                if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+                a.image[fi] = __fadd_rn(a.image[fi], inc);
+            }
+        } else if (s.field16 != nullptr) {
+            float F = load16x1(s.field16, fi, a.kind16, __ldg(s.field_iscale));
+            if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
+            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
+            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+            kahan(a.image[fi], a.comp[fi], inc);
+        }
+    }
+}
+
+// Tile bounds of generic rect r, tile t: an even split of the rect into
+// r_tz x r_tx tiles.
+__host__ __device__ __forceinline__ void generic_bounds(const PairArgs& P, int r, int t, int* z0, int* z1, int* x0,
+                                                        int* x1) {
+    const int nz = P.r_tz[r], nxr = P.r_tx[r];
+    const int tz = t % nz, tx = t / nz;
+    *z0 = P.r_zd0[r] + (tz * P.r_h[r]) / nz;
+    *z1 = P.r_zd0[r] + ((tz + 1) * P.r_h[r]) / nz;
+    *x0 = P.r_x0[r] + (tx * P.r_w[r]) / nxr;
+    *x1 = P.r_x0[r] + ((tx + 1) * P.r_w[r]) / nxr;
+}
+
+template <int MODE>
+__device__ __forceinline__ void pair_generic_tile(const PairArgs& P, float* sm, int r, int t, int b) {
+    const StepArgs& a = P.a;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    GenTile G;
+    generic_bounds(P, r, t, &G.z0, &G.z1, &G.x0, &G.x1);
+    G.S0 = sm;
+    G.S1 = G.S0 + GH0 * GW0;
+    G.F1x = G.S1 + GH1 * GW1;
+    G.F1z = G.F1x + GH1 * GW1;
+    G.X1x = G.F1z + GH1 * GW1;
+    G.X1z = G.X1x + GH1 * GW1;
+    G.SD1 = G.X1z + GH1 * GW1;
+    const int H = G.z1 - G.z0, W = G.x1 - G.x0;
+    const int H0 = H + 12, W0 = W + 12;
+    for (int i = tid; i < H0 * W0; i += NT) {
+        const int xl = i / H0, zl = i - xl * H0;
+        const int zd = G.z0 - 6 + zl, x = G.x0 - 6 + xl;
+        G.S0[xl * GH0 + zl] = (zd >= 0 && zd < a.ldz && x >= 0 && x < a.nxt) ? a.p[(size_t)x * a.ldz + zd] : 0.f;
+    }
+    __syncthreads();
+    const int H1 = H + 6, W1 = W + 6;
+    for (int i = tid; i < H1 * W1; i += NT) {
+        const int xl = i / H1, zl = i - xl * H1;
+        pair_cell<MODE, 0>(P, G, G.z0 - 3 + zl, G.x0 - 3 + xl);
+    }
+    if (P.nsub == 2) {
+        __syncthreads();
+        for (int i = tid; i < H * W; i += NT) {
+            const int xl = i / H, zl = i - xl * H;
+            pair_cell<MODE, 1>(P, G, G.z0 + zl, G.x0 + xl);
+        }
+    }
+    if (MODE == 0 && P.rec_first != nullptr)
+        gather_receivers(P, b, G.S0, G.z0 - 6, G.x0 - 6, GH0, G.S1, G.z0 - 3, G.x0 - 3, GH1);
+}
+
+// Tile b of a launch; false if its bulk copies did not complete.
+template <int MODE>
+__device__ __forceinline__ bool pair_tile(const PairArgs& P, float* sm, uint64_t* bar, uint32_t& phase, int b) {
+    int r = 0;
+    while (r + 1 < P.nrect && b >= P.r_first[r + 1]) ++r;
+    const int t = b - P.r_first[r];
+    if (P.r_type[r] == 0) return pair_clean_tile<MODE>(P, sm, bar, phase, r, t, b);
+    pair_generic_tile<MODE>(P, sm, r, t, b);
+    return true;
+}
+
+__device__ __forceinline__ void pair_prologue_convert(const PairArgs& P, int tid) {
+    const StepArgs& a = P.a;
+    if (a.q_src != nullptr) quantize_part(a.q_src, a.q_amax, a.q_dst, a.q_iscale, a.q_n, a.kind16, tid);
+    if (P.q_src2 != nullptr) quantize_part(P.q_src2, P.q_amax2, P.q_dst2, P.q_iscale2, P.q_n2, a.kind16, tid);
+}
+
+__device__ __forceinline__ void pair_flush_amax(const PairArgs& P) {
+    for (int k = 0; k < 2; ++k)
+        if (P.sub[k].field_amax != nullptr && s_pair_amax[k] != 0u) atomicMax(P.sub[k].field_amax, s_pair_amax[k]);
+    s_pair_amax[0] = s_pair_amax[1] = 0u;
+}
+
+// Two steps (or one) of one shot.  Persistent blocks take tiles from this
+// launch's counter (clean tiles first); the other counter is cleared for
+// the next launch.
+template <int MODE>
+__global__ void __launch_bounds__(NT, 5) pair_kernel(const PairArgs P) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int tile_id;
+    const StepArgs& a = P.a;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    grid_dependency_wait();
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        s_pair_amax[0] = s_pair_amax[1] = 0u;
+    }
+    if (MODE == 0) pair_prologue_convert(P, tid);
+    if (blockIdx.x == 0 && tid == 0) a.tile_counter[a.counter_sel ^ 1] = 0;
+    __syncthreads();
+    uint32_t phase = 0;
+    const int total = P.r_first[P.nrect];
+    for (;;) {
+        if (tid == 0) tile_id = atomicAdd(a.tile_counter + a.counter_sel, 1);
+        __syncthreads();
+        const int b = tile_id;
+        if (b >= total) {
+            if (MODE == 0 && tid == 0) pair_flush_amax(P);
+            return;
+        }
+        if (!pair_tile<MODE>(P, sm, &bar, phase, b)) return;
+        __syncthreads();  // shared tiles and tile_id are reused
+    }
+}
+
+// Two steps (or one) of several shots in one launch; see PairBatchParams.
+// A slot's arguments are copied into shared memory when a block switches
+// slot.  FIXED >= 0 is the instance for a launch whose slots are all in
+// pass FIXED.
+template <int FIXED>
+__global__ void __launch_bounds__(NT, 5) pair_batch_kernel(const PairBatchParams bp) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int tile_id;
+    __shared__ __align__(16) PairArgs sa;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    grid_dependency_wait();
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        s_pair_amax[0] = s_pair_amax[1] = 0u;
+    }
+    for (int s = 0; s < bp.nslots; ++s) {
+        if (FIXED > 0 || bp.mode[s] != 0) continue;
+        const PairArgs* g = bp.args[s];
+        const StepArgs& ga = g->a;
+        if (ga.q_src != nullptr) quantize_part(ga.q_src, ga.q_amax, ga.q_dst, ga.q_iscale, ga.q_n, ga.kind16, tid);
+        if (g->q_src2 != nullptr)
+            quantize_part(g->q_src2, g->q_amax2, g->q_dst2, g->q_iscale2, g->q_n2, ga.kind16, tid);
+    }
+    if (blockIdx.x == 0 && tid == 0) bp.counter[bp.counter_sel ^ 1] = 0;
+    __syncthreads();
+    uint32_t phase = 0;
+    int cur = -1;
+    const int total = bp.first[bp.nslots];
+    constexpr int kWords = (int)(sizeof(PairArgs) / sizeof(long long));
+    static_assert(sizeof(PairArgs) % sizeof(long long) == 0, "PairArgs is copied in 8-byte words");
+    for (;;) {
+        if (tid == 0) tile_id = atomicAdd(bp.counter + bp.counter_sel, 1);
+        __syncthreads();
+        const int b = tile_id;
+        if (b >= total) {
+            if (tid == 0 && cur >= 0 && bp.mode[cur] == 0) pair_flush_amax(sa);
+            return;
+        }
+        int s = 0;
+        while (s + 1 < bp.nslots && b >= bp.first[s + 1]) ++s;
+        if (s != cur) {  // every thread takes the same branch
+            if (tid == 0 && cur >= 0 && bp.mode[cur] == 0) pair_flush_amax(sa);
+            __syncthreads();  // the flush reads sa before it is replaced
+            const long long* src = reinterpret_cast<const long long*>(bp.args[s]);
+            long long* dst = reinterpret_cast<long long*>(&sa);
+            for (int i = tid; i < kWords; i += NT) dst[i] = src[i];
+            __syncthreads();
+            cur = s;
+        }
+        const int lb = b - bp.first[s];
+        bool ok;
+        if (FIXED >= 0) {
+            ok = pair_tile<(FIXED >= 0 ? FIXED : 0)>(sa, sm, &bar, phase, lb);
+        } else {
+            const int md = bp.mode[s];
+            ok = md == 0 ? pair_tile<0>(sa, sm, &bar, phase, lb)
+                         : (md == 1 ? pair_tile<1>(sa, sm, &bar, phase, lb) : pair_tile<2>(sa, sm, &bar, phase, lb));
+        }
+        if (!ok) return;
+        __syncthreads();  // shared tiles, tile_id and (next switch) sa are reused
+    }
+}
+
+constexpr int kPairSmemBytes = kPairFloats * (int)sizeof(float);
+
+template <int MODE>
+int pair_blocks_per_sm() {
+    static int nb = 0;
+    if (nb == 0) {
+        cudaFuncSetAttribute(pair_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmemBytes);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pair_kernel<MODE>, NT, kPairSmemBytes);
+        nb = n > 0 ? n : 1;
+    }
+    return nb;
+}
+
+template <int FIXED>
+int pair_batch_blocks_per_sm() {
+    static int nb = 0;
+    if (nb == 0) {
+        cudaFuncSetAttribute(pair_batch_kernel<FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmemBytes);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pair_batch_kernel<FIXED>, NT, kPairSmemBytes);
+        nb = n > 0 ? n : 1;
+    }
+    return nb;
+}
+
+template <class K, class A>
+int launch_persistent(K kernel, const A& args, int tiles, int blocks, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(std::min(tiles, blocks));
+    cfg.blockDim = dim3(32, NWARP);
+    cfg.dynamicSmemBytes = (size_t)kPairSmemBytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, kernel, args);
+}
+
+}  // namespace
+
+int prepare_pair_kernels() {
+    return (pair_blocks_per_sm<0>() > 0 && pair_blocks_per_sm<1>() > 0 && pair_blocks_per_sm<2>() > 0 &&
+            pair_batch_blocks_per_sm<-1>() > 0 && pair_batch_blocks_per_sm<0>() > 0 &&
+            pair_batch_blocks_per_sm<1>() > 0 && pair_batch_blocks_per_sm<2>() > 0)
+               ? (int)cudaGetLastError()
+               : 1;
+}
+
+int launch_pair(int mode, const PairArgs& P, void* stream) {
+    const int tiles = P.r_first[P.nrect];
+    if (tiles <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int sms = P.a.num_sms;
+    if (mode == 0) return launch_persistent(pair_kernel<0>, P, tiles, sms * pair_blocks_per_sm<0>(), st);
+    if (mode == 1) return launch_persistent(pair_kernel<1>, P, tiles, sms * pair_blocks_per_sm<1>(), st);
+    return launch_persistent(pair_kernel<2>, P, tiles, sms * pair_blocks_per_sm<2>(), st);
+}
+
+int launch_pair_batch(const PairBatchParams& bp, int num_sms, void* stream) {
+    const int tiles = bp.first[bp.nslots];
+    if (bp.nslots <= 0 || tiles <= 0) return 0;
+    bool same = true;
+    for (int s = 1; s < bp.nslots; ++s) same = same && bp.mode[s] == bp.mode[0];
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!same) return launch_persistent(pair_batch_kernel<-1>, bp, tiles, num_sms * pair_batch_blocks_per_sm<-1>(), st);
+    if (bp.mode[0] == 0)
+        return launch_persistent(pair_batch_kernel<0>, bp, tiles, num_sms * pair_batch_blocks_per_sm<0>(), st);
+    if (bp.mode[0] == 1)
+        return launch_persistent(pair_batch_kernel<1>, bp, tiles, num_sms * pair_batch_blocks_per_sm<1>(), st);
+    return launch_persistent(pair_batch_kernel<2>, bp, tiles, num_sms * pair_batch_blocks_per_sm<2>(), st);
+}
+
+bool plan_pair(PairArgs* P, const int* row_slot_host) {
+    const StepArgs& a = P->a;
+    P->txc = TXC;
+    const int dn = a.dn, ny = a.ny, nx = a.nx, nyt = a.nyt, nxt = a.nxt, zoff = a.zoff;
+    // Clean rows (logical): the tile and its 3-row ring are interior rows,
+    // at least 4 rows below a free surface and 4 rows from every row that
+    // holds an injection point.
+    std::vector<char> ok(nyt, 0);
+    for (int z = dn + 3; z < dn + ny - 3; ++z) ok[z] = 1;
+    if (a.fs)
+        for (int z = dn; z <= dn + 3 && z < nyt; ++z) ok[z] = 0;
+    if (row_slot_host)
+        for (int zd = 0; zd < a.ldz; ++zd)
+            if (row_slot_host[zd] >= 0)
+                for (int z = zd - zoff - 3; z <= zd - zoff + 3; ++z)
+                    if (z >= 0 && z < nyt) ok[z] = 0;
+    const int cx0 = dn + 3, cx1 = dn + nx - 3;
+    std::vector<std::pair<int, int>> runs;  // device rows, both ends multiples of 4
+    if (cx1 > cx0)
+        for (int z = 0; z < nyt;) {
+            if (!ok[z]) {
+                ++z;
+                continue;
+            }
+            int e = z;
+            while (e < nyt && ok[e]) ++e;
+            const int ds = (z + zoff + 3) / 4 * 4, de = (e + zoff) / 4 * 4;
+            if (de - ds >= 4) runs.push_back({ds, de});
+            z = e;
+        }
+    if (runs.size() > 4) {  // many injection rows: keep the four longest clean runs
+        std::sort(runs.begin(), runs.end(),
+                  [](const std::pair<int, int>& u, const std::pair<int, int>& v) {
+                      return u.second - u.first > v.second - v.first;
+                  });
+        runs.resize(4);
+        std::sort(runs.begin(), runs.end());
+    }
+    // Band cuts (device rows): live rows, strip edges, clean runs.
+    const int top = (a.fs ? dn : 0) + zoff, bot = nyt + zoff;
+    std::vector<int> cuts = {top, dn + zoff, dn + ny + zoff, bot};
+    for (auto& rn : runs) {
+        cuts.push_back(rn.first);
+        cuts.push_back(rn.second);
+    }
+    std::sort(cuts.begin(), cuts.end());
+    cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+    int n = 0;
+    bool overflow = false;
+    P->r_first[0] = 0;
+    auto add = [&](int type, int zd0, int x0, int h, int w) {
+        if (h <= 0 || w <= 0) return;
+        if (n >= kPairRects) {
+            overflow = true;
+            return;
+        }
+        P->r_type[n] = type;
+        P->r_zd0[n] = zd0;
+        P->r_x0[n] = x0;
+        P->r_h[n] = h;
+        P->r_w[n] = w;
+        P->r_tz[n] = type == 0 ? (h + TZC - 1) / TZC : (h + GZ - 1) / GZ;
+        P->r_tx[n] = type == 0 ? (w + TXC - 1) / TXC : (w + GX - 1) / GX;
+        P->r_first[n + 1] = P->r_first[n] + P->r_tz[n] * P->r_tx[n];
+        ++n;
+    };
+    for (auto& rn : runs) add(0, rn.first, cx0, rn.second - rn.first, cx1 - cx0);
+    for (size_t i = 0; i + 1 < cuts.size(); ++i) {
+        const int za = cuts[i], zb = cuts[i + 1];
+        if (za < top || zb > bot) continue;
+        bool clean = false;
+        for (auto& rn : runs) clean = clean || (rn.first == za && rn.second == zb);
+        add(1, za, 0, zb - za, dn);
+        if (clean) {
+            add(1, za, dn, zb - za, cx0 - dn);
+            add(1, za, cx1, zb - za, dn + nx - cx1);
+        } else {
+            add(1, za, dn, zb - za, nx);
+        }
+        add(1, za, dn + nx, zb - za, nxt - (dn + nx));
+    }
+    P->nrect = n;
+    return !overflow;
+}
+
+void pair_tile_rect(const PairArgs& P, int b, int* z0, int* z1, int* x0, int* x1) {
+    int r = 0;
+    while (r + 1 < P.nrect && b >= P.r_first[r + 1]) ++r;
+    const int t = b - P.r_first[r];
+    if (P.r_type[r] == 0) {
+        const int tz = t % P.r_tz[r], tx = t / P.r_tz[r];
+        *z0 = P.r_zd0[r] + tz * TZC;
+        *x0 = P.r_x0[r] + tx * P.txc;
+        *z1 = std::min(*z0 + TZC, P.r_zd0[r] + P.r_h[r]);
+        *x1 = std::min(*x0 + P.txc, P.r_x0[r] + P.r_w[r]);
+    } else {
+        generic_bounds(P, r, t, z0, z1, x0, x1);
+    }
+}
+
+void pair_rec_lists(const PairArgs& P, int nrec, const int* h_rec_cell, std::vector<int>* first,
+                    std::vector<int>* idx) {
+    const int n = P.r_first[P.nrect];
+    std::vector<std::vector<int>> by(n);
+    std::vector<int> R(4 * (size_t)n);
+    for (int b = 0; b < n; ++b) pair_tile_rect(P, b, &R[4 * b], &R[4 * b + 1], &R[4 * b + 2], &R[4 * b + 3]);
+    for (int i = 0; i < nrec; ++i) {
+        const int x = h_rec_cell[i] / P.a.ldz, zd = h_rec_cell[i] % P.a.ldz;
+        for (int b = 0; b < n; ++b)
+            if (zd >= R[4 * b] && zd < R[4 * b + 1] && x >= R[4 * b + 2] && x < R[4 * b + 3]) {
+                by[b].push_back(i);
+                break;
+            }
+    }
+    first->assign(n + 1, 0);
+    idx->clear();
+    for (int b = 0; b < n; ++b) {
+        idx->insert(idx->end(), by[b].begin(), by[b].end());
+        (*first)[b + 1] = (int)idx->size();
+    }
+}
+
+}  // namespace psdm

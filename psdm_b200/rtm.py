@@ -223,6 +223,10 @@ class Engine:
         """psdm_engine_set_pass_launch: one cooperative launch per pass (True) or one launch per step."""
         L.check(L.lib().psdm_engine_set_pass_launch(self._h, int(bool(on))))
 
+    def set_steps_per_launch(self, steps: int):
+        """psdm_engine_set_steps_per_launch: 2 (default) time steps per kernel launch, or 1."""
+        L.check(L.lib().psdm_engine_set_steps_per_launch(self._h, int(steps)))
+
     def set_checkpointing(self, interval: int):
         """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
         L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))
