@@ -46,6 +46,7 @@ sys.path.insert(0, ROOT)
 
 # ---- workload (config 2) --------------------------------------------------
 NY, NX, DD, DT, NT, DPML, F0 = 1200, 4000, 6.25, 5e-4, 8000, 50, 20.0
+CPU_SAMPLE_STEPS = 200  # forward and backward steps per CPU shot sample
 ADDED_SPACE = 500.0
 WORKLOAD = "rtm_config2_1200x4000_dx6.25_nt8000_cpml50_480ch_fp32"
 
@@ -76,6 +77,17 @@ def algorithmic_bytes(ny, nx_w, dpml, fs=1):
     g = grid_cells(ny, nx_w, dpml, fs)
     base = 16 * g["n_act"] + 16 * (g["n_xpml"] + g["n_zpml"])
     return base + 4 * g["n_int"], base + 12 * g["n_int"], g
+
+
+def algorithmic_bytes_mixed(ny, nx_w, dpml, fs, ks):
+    """Compulsory bytes of one step of the mixed-precision form: the FP32
+    propagation's 16 B per updated cell and C-PML bytes, and per interior
+    cell every ks steps the staged FP32 snapshot (written, read back) and its
+    16-bit copy (forward), or the 16-bit snapshot and the image and
+    compensation read-modify-writes (backward)."""
+    g = grid_cells(ny, nx_w, dpml, fs)
+    base = 16 * g["n_act"] + 16 * (g["n_xpml"] + g["n_zpml"])
+    return base + 10 * g["n_int"] / ks, base + 18 * g["n_int"] / ks, g
 
 
 def profiled_traffic(which: str):
@@ -146,7 +158,9 @@ class ClockSampler:
 # ---- CPU arm (oracle restatement) -------------------------------------------
 
 def _cpu_worker(args):
-    """One process = one shot sample of the CPU restatement (C2 window, nt_s steps)."""
+    """One process = one shot sample of the CPU restatement: the first nt_s
+    forward and nt_s backward steps of a config-2 shot on the config-2
+    migration model window (1200 x 1136 cells)."""
     nt_s, seed = args
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
@@ -154,7 +168,7 @@ def _cpu_worker(args):
     sv = synth.config2_survey(4)
     s = seed % sv.nshots
     nx_w, x_i, x_f = O.dynamic_window(int(sv.nxSou[s]), sv.nxRec[s], DD, NX, ADDED_SPACE)
-    vp = np.full((nx_w, NY), 2000.0, dtype=np.float32)
+    vp = np.ascontiguousarray(synth.smooth_model(synth_model_cached(), 100.0, DD)[x_i - 1:x_f])
     src = O.ricker_mcs(nt_s, DT, F0)
     tgt = np.random.default_rng(seed).standard_normal((sv.nrec, nt_s)).astype(np.float32)
     t0 = time.perf_counter()
@@ -201,7 +215,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     procs = cpu_procs(64)
-    nt_s = 12
+    nt_s = CPU_SAMPLE_STEPS
     vals = []
     for i in range(args.warmup + args.steps):
         r = cpu_sample(procs, nt_s)
@@ -209,14 +223,16 @@ def run_reference(args):
             vals.append(r)
     v = statistics.median([r["shots_per_s"] for r in vals])
     sample = (f"{procs} processes x one config-2 shot sample each ({nt_s} forward + {nt_s} backward steps on "
-              f"the {NY}x{vals[0]['nx_w']} window), extrapolated to nt={NT}")
+              f"the {NY}x{vals[0]['nx_w']} window of the migration model), extrapolated to nt={NT}; "
+              f"{host_cores()} host cores")
     line = {"impl": "reference", "metric": "rtm_shots_per_s", "value": v, "unit": "shots/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cpu": "reference algorithm, C++ restatement (oracle/)",
                        "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": v, "unit": "shots/s", "cores": procs, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "shots/s", "cores": procs, "kind": "port", "sample": sample,
+                             "host_cores": host_cores(), "processes": procs},
             "e2e": {"value": v, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -224,16 +240,18 @@ def run_reference(args):
 
 # ---- GPU arm -----------------------------------------------------------------
 
-# The engine's other forms, timed after the drop-in on the same shots:
-# (name, precision, store_snap, slots); slots = 0 is one shot at a time
-# through psdm_rtm_shot_device, otherwise psdm_rtm_batch_device with that
-# many shots in flight.  precision 1 / 2 = binary16 / bfloat16 snapshots.
+# The engine's other forms, timed after the drop-in on the same shots.
+# slots = 0 is one shot at a time through psdm_rtm_shot_device, otherwise
+# psdm_rtm_batch_device with that many shots in flight; precision 1 / 2 =
+# binary16 / bfloat16 snapshots every ks steps; ckpt = checkpoint interval of
+# FP32 shots; spl = time steps per kernel launch.
 FORMS = [
-    ("fp16_ks4", 1, 4, 0),
-    ("batch_fp16_ks4", 1, 4, 8),
-    ("batch_bf16_ks4", 2, 4, 8),
-    ("batch_fp32", 0, 1, 2),
-    ("fp32_checkpoint_k100", 0, 1, -100),  # slots < 0: one shot at a time, checkpoint interval -slots
+    dict(name="fp32_one_step", precision=0, ks=1, slots=0, spl=1),
+    dict(name="fp16_ks4", precision=1, ks=4, slots=0),
+    dict(name="batch_fp16_ks4", precision=1, ks=4, slots=8),
+    dict(name="batch_bf16_ks4", precision=2, ks=4, slots=8),
+    dict(name="batch_fp32", precision=0, ks=1, slots=2),
+    dict(name="fp32_checkpoint_k100", precision=0, ks=1, slots=0, ckpt=100),
 ]
 
 
@@ -313,14 +331,15 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
     from psdm_b200 import rtm
     out = {}
     outs = [torch.zeros((it["nx_w"], NY), dtype=torch.float32, device=dev) for it in items]
-    for name, precision, ks, slots in FORMS:
+    for f in FORMS:
+        name, precision, ks, slots = f["name"], f["precision"], f["ks"], f["slots"]
         if name not in names:
             continue
         prm = rtm.Params(dPML=DPML, fs=1, strategy=1, precision=precision)
-        ckpt = -slots if slots < 0 else 0
-        slots = max(slots, 0)
+        ckpt = f.get("ckpt", 0)
         n = 2 * slots if slots else 4
         engine.set_checkpointing(ckpt)
+        engine.set_steps_per_launch(f.get("spl", 2))
         sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
 
         def run(k):
@@ -344,12 +363,196 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         engine.set_checkpointing(0)
+        engine.set_steps_per_launch(2)
         v = n / (e0.elapsed_time(e1) / 1e3)
         out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
                      "slots": engine.batch_slots() if slots else 1, "precision": ["f32", "fp16", "bf16"][precision],
                      "store_snap": ks}
         if ckpt:
             out[name]["checkpoint_interval"] = ckpt
+        if f.get("spl", 2) != 2:
+            out[name]["steps_per_launch"] = f["spl"]
+    return out
+
+
+def _shot_rate(torch, dev, stream, run, nshots):
+    """Shots/s of run() (warm-up call first), CUDA events on `stream`."""
+    run()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return nshots / (e0.elapsed_time(e1) / 1e3)
+
+
+def _config_line(name, rate, shots, cells_steps, bytes_per_shot, peak, **extra):
+    """A config entry: shots/s, Gcell-updates/s and the achieved HBM rate on
+    the algorithmic bytes, against the measured copy bandwidth."""
+    gbs = bytes_per_shot * rate / 1e9
+    d = {"shots_per_s": rate, "shots": shots, "gcell_upd_per_s": cells_steps * rate / 1e9,
+         "achieved_gbs": gbs, "frac_of_peak": gbs / peak}
+    d.update(extra)
+    return d
+
+
+def time_config1(engine, torch, dev, stream, peak, with_cpu):
+    """Config 1 in full: its 4 shots (200 x 600 at 10 m, CPML 40, nt 3000,
+    120 channels), plain FP32 one shot at a time and all 4 in flight; and the
+    CPU restatement running the 4 shots in parallel processes."""
+    from oracle import oracle as O
+    from psdm_b200 import rtm, synth
+    ny, nx, dd, dt, nt, dpml, f0 = 200, 600, 10.0, 1e-3, 3000, 40, 15.0
+    sv = synth.config1_survey()
+    vt = synth.config1_model(seed=1)
+    vm = synth.smooth_model(vt, 100.0, dd)
+    prm = rtm.Params(dPML=dpml, fs=0, strategy=1)
+    src = rtm.ricker_mcs(nt, dt, f0)
+    d_src = torch.from_numpy(src).to(dev)
+    items = []
+    for s in range(sv.nshots):
+        nxS, nyS, nxR, nyR = int(sv.nxSou[s]), int(sv.nySou[s]), sv.nxRec[s], sv.nyRec[s]
+        nx_w, x_i, x_f = rtm.dynamic_window(nxS, nxR, dd, nx, ADDED_SPACE)
+        obs = engine.model_shot(prm, nxS, nyS, nxR, nyR, src, dd, dt, ny, nx, nx_w,
+                                np.ascontiguousarray(vt[x_i - 1:x_f]), ADDED_SPACE, nt)
+        obs = synth.mute_direct(obs, sv.pos_rec[s] - sv.pos_shot[s], dt)
+        vmw = np.ascontiguousarray(vm[x_i - 1:x_f])
+        items.append(dict(nxSou=nxS, nySou=nyS, nxRec=nxR, nyRec=nyR, nx_w=nx_w, vm=vmw, obs=obs,
+                          d_vp=torch.from_numpy(vmw).to(dev), d_obs=torch.from_numpy(obs).to(dev),
+                          d_img=torch.zeros((nx_w, ny), dtype=torch.float32, device=dev)))
+
+    def one_at_a_time():
+        for it in items:
+            engine.rtm_shot_device(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], d_src.data_ptr(),
+                                   it["d_obs"].data_ptr(), dd, dt, ny, nx, it["nx_w"], it["d_vp"].data_ptr(),
+                                   ADDED_SPACE, 1, nt, nt, nt, 0, 1, 0, it["d_img"].data_ptr())
+
+    def batched():
+        descs = [dict(nxSou=it["nxSou"], nySou=it["nySou"], nxRec=it["nxRec"], nyRec=it["nyRec"], nx_w=it["nx_w"],
+                      nt_prop2=nt, nt_taper=nt, d_Vp_w=it["d_vp"].data_ptr(), d_Data_target=it["d_obs"].data_ptr(),
+                      d_PSDM_w=it["d_img"].data_ptr()) for it in items]
+        engine.rtm_batch_device(prm, descs, d_src.data_ptr(), dd, dt, ny, nx, ADDED_SPACE, store_snap=1,
+                                max_slots=len(items))
+
+    fb, bb, g = algorithmic_bytes(ny, items[0]["nx_w"], dpml, 0)
+    cells = 2 * (nt - 1) * g["n_pad"]
+    out = {"workload": "rtm_config1_200x600_dx10_nt3000_cpml40_120ch_fp32_4shots"}
+    out["gpu_one_at_a_time"] = _config_line("config1", _shot_rate(torch, dev, stream, one_at_a_time, len(items)),
+                                            len(items), cells, (fb + bb) * (nt - 1), peak)
+    out["gpu_batched_4"] = _config_line("config1", _shot_rate(torch, dev, stream, batched, len(items)), len(items),
+                                        cells, (fb + bb) * (nt - 1), peak)
+    if with_cpu:
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(len(items)) as pool:
+            pool.map(_cpu_config1_worker, [(it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], it["vm"], it["obs"])
+                                           for it in items])
+        wall = time.perf_counter() - t0
+        out["cpu"] = {"shots_per_s": len(items) / wall, "processes": len(items), "host_cores": host_cores(),
+                      "kind": "port", "sample": "the 4 shots in full, one process each (includes process start)"}
+    return out
+
+
+def _cpu_config1_worker(args):
+    nxS, nyS, nxR, nyR, vm, obs = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    nt = obs.shape[1]
+    src = O.ricker_mcs(nt, 1e-3, 15.0)
+    O.rtm_shot(dPML=40, fs=0, nxSou=nxS, nySou=nyS, nxRec=nxR, nyRec=nyR, Data_source=src, Data_target=obs, dd=10.0,
+               dt=1e-3, nx=600, vp_w=vm, added_space=ADDED_SPACE, store_snap=1, nt_snap=nt, nt_prop2=nt, nt_taper=nt)
+    return 0
+
+
+def time_config4(engine, torch, dev, stream, peak, nshots=24):
+    """Config 4: a seeded subset of the 1000 uneven shots (windows of 800-2400
+    cells, records of 4000-10000 steps) on the 1500 x 12000 model, batched
+    with binary16 snapshots every 4 steps (psdm_rtm_batch_device, slots sized
+    to the free device memory)."""
+    from psdm_b200 import rtm, synth
+    ny, nx, dd, dt, dpml, f0 = 1500, 12000, 6.25, 5e-4, 50, 20.0
+    shots = synth.config4_shots()[:nshots]
+    vt = synth.config4_model(seed=4)
+    vm = synth.smooth_model(vt, 100.0, dd)
+    ntmax = max(s["nt"] for s in shots)
+    src = rtm.ricker_mcs(ntmax, dt, f0)
+    d_src = torch.from_numpy(src).to(dev)
+    prm32 = rtm.Params(dPML=dpml, fs=1, strategy=1)
+    descs, keep, cells, nbytes = [], [], 0, 0.0
+    for s in shots:
+        nx_w, x_i, x_f = rtm.dynamic_window(s["nxSou"], s["nxRec"], dd, nx, ADDED_SPACE)
+        obs = engine.model_shot(prm32, s["nxSou"], s["nySou"], s["nxRec"], s["nyRec"], src[:s["nt"]], dd, dt, ny, nx,
+                                nx_w, np.ascontiguousarray(vt[x_i - 1:x_f]), ADDED_SPACE, s["nt"])
+        obs = synth.mute_direct(obs, s["pos_rec"] - s["pos_shot"], dt)
+        d_vp = torch.from_numpy(np.ascontiguousarray(vm[x_i - 1:x_f])).to(dev)
+        d_obs = torch.from_numpy(obs).to(dev)
+        d_img = torch.zeros((nx_w, ny), dtype=torch.float32, device=dev)
+        keep += [d_vp, d_obs, d_img]
+        descs.append(dict(nxSou=s["nxSou"], nySou=s["nySou"], nxRec=s["nxRec"], nyRec=s["nyRec"], nx_w=nx_w,
+                          nt_prop2=s["nt"], nt_taper=s["nt"], d_Vp_w=d_vp.data_ptr(), d_Data_target=d_obs.data_ptr(),
+                          d_PSDM_w=d_img.data_ptr()))
+        fb, bb, g = algorithmic_bytes_mixed(ny, nx_w, dpml, 1, 4)
+        cells += 2 * (s["nt"] - 1) * g["n_pad"]
+        nbytes += (fb + bb) * (s["nt"] - 1)
+    engine.trim()
+    prm = rtm.Params(dPML=dpml, fs=1, strategy=1, precision=1)
+    run = lambda: engine.rtm_batch_device(prm, descs, d_src.data_ptr(), dd, dt, ny, nx, ADDED_SPACE, store_snap=4,
+                                          max_slots=16)
+    rate = _shot_rate(torch, dev, stream, run, len(descs))
+    widths = [d["nx_w"] for d in descs]
+    line = _config_line("config4", rate, len(descs), cells / len(descs), nbytes / len(descs), peak,
+                        form="batched, binary16 snapshots every 4 steps", slots=engine.batch_slots(),
+                        nx_w_range=[min(widths), max(widths)], nt_range=[min(s["nt"] for s in shots),
+                                                                        max(s["nt"] for s in shots)])
+    del keep
+    engine.trim()
+    return {"workload": f"rtm_config4_1500x12000_dx6.25_{len(descs)}_of_1000_uneven_shots", "batch_fp16_ks4": line}
+
+
+def time_config5(engine, torch, dev, stream, peak):
+    """Config 5: one shot of the 3000 x 16000 model at 5 m (dt 0.4 ms, nt
+    12000, 960 channels, 12 km streamer): FP32 snapshots (377 GB) do not fit,
+    so the forms are binary16 snapshots every 4 steps and FP32 with
+    checkpoints every 100 steps."""
+    from psdm_b200 import rtm, synth
+    ny, nx, dd, dt, nt, dpml, f0 = 3000, 16000, 5.0, 4e-4, 12000, 50, 25.0
+    sv = synth.config5_survey(1)
+    nxS, nyS, nxR, nyR = int(sv.nxSou[0]), int(sv.nySou[0]), sv.nxRec[0], sv.nyRec[0]
+    nx_w, x_i, x_f = rtm.dynamic_window(nxS, nxR, dd, nx, ADDED_SPACE)
+    vt = synth.config5_model(seed=5, nx=x_f)
+    vm = synth.smooth_model(vt, 100.0, dd)
+    src = rtm.ricker_mcs(nt, dt, f0)
+    d_src = torch.from_numpy(src).to(dev)
+    prm32 = rtm.Params(dPML=dpml, fs=1, strategy=1)
+    engine.trim()
+    obs = engine.model_shot(prm32, nxS, nyS, nxR, nyR, src, dd, dt, ny, nx, nx_w,
+                            np.ascontiguousarray(vt[x_i - 1:x_f]), ADDED_SPACE, nt)
+    obs = synth.mute_direct(obs, sv.pos_rec[0] - sv.pos_shot[0], dt)
+    d_vp = torch.from_numpy(np.ascontiguousarray(vm[x_i - 1:x_f])).to(dev)
+    d_obs = torch.from_numpy(obs).to(dev)
+    d_img = torch.zeros((nx_w, ny), dtype=torch.float32, device=dev)
+    out = {"workload": f"rtm_config5_3000x16000_dx5_nt12000_cpml50_960ch_window{nx_w}"}
+    for name, precision, ks, ckpt in (("fp16_ks4", 1, 4, 0), ("fp32_checkpoint_k100", 0, 1, 100)):
+        prm = rtm.Params(dPML=dpml, fs=1, strategy=1, precision=precision)
+        engine.set_checkpointing(ckpt)
+        run = lambda: engine.rtm_shot_device(prm, nxS, nyS, nxR, nyR, d_src.data_ptr(), d_obs.data_ptr(), dd, dt, ny,
+                                             nx, nx_w, d_vp.data_ptr(), ADDED_SPACE, ks, nt, nt, nt, 0, 1, 0,
+                                             d_img.data_ptr())
+        try:
+            rate = _shot_rate(torch, dev, stream, run, 1)
+        finally:
+            engine.set_checkpointing(0)
+        if precision:
+            fb, bb, g = algorithmic_bytes_mixed(ny, nx_w, dpml, 1, ks)
+            nbytes = (fb + bb) * (nt - 1)
+        else:  # the forward pass runs twice
+            fb, bb, g = algorithmic_bytes(ny, nx_w, dpml, 1)
+            nbytes = (2 * fb + bb) * (nt - 1)
+        cells = 2 * (nt - 1) * g["n_pad"]
+        out[name] = _config_line("config5", rate, 1, cells, nbytes, peak)
+        engine.trim()
+    out["fp32_all_snapshots"] = {"fits": False, "snapshot_gb": round(4.0 * ny * nx_w * (nt - 1) / 1e9, 1)}
     return out
 
 
@@ -482,19 +685,34 @@ def run_gpu(args):
                "d2h_bytes_per_step": int(d2h), "api": "psdm_rtm_shot (C ABI, pinned host buffers)"}
 
     forms = None
-    names = [f[0] for f in FORMS] if args.forms == "all" else [n for n in args.forms.split(",") if n and n != "none"]
+    names = [f["name"] for f in FORMS] if args.forms == "all" else [n for n in args.forms.split(",") if n and n != "none"]
     if world == 1 and names:
         forms = time_forms(engine, torch, dev, stream, d_src, items_u, names, value)
+    configs = None
+    cnames = ["config1", "config4", "config5"] if args.configs == "all" else \
+        [n for n in args.configs.split(",") if n and n != "none"]
+    if world == 1 and cnames:
+        peak_c, _ = _peaks()
+        configs = {}
+        if "config1" in cnames:
+            configs["config1"] = time_config1(engine, torch, dev, stream, peak_c, not args.no_cpu)
+        if "config4" in cnames:
+            configs["config4"] = time_config4(engine, torch, dev, stream, peak_c)
+        if "config5" in cnames:
+            configs["config5"] = time_config5(engine, torch, dev, stream, peak_c)
     conditioning = None
     if rank == 0 and world == 1 and not args.no_cpu:
         conditioning = time_conditioning(engine, torch, dev, stream, survey)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_sample(cpu_procs(32), 12)
-        cpu = {"value": r["shots_per_s"], "unit": "shots/s", "cores": cpu_procs(32), "kind": "port",
-               "sample": f"{cpu_procs(32)} processes x one config-2 shot sample each (12 forward + 12 backward "
-                         f"steps of the C++ restatement), extrapolated to nt={NT}; {r['sec_per_shot']:.0f} s/shot"}
+        procs = cpu_procs(32)
+        r = cpu_sample(procs, CPU_SAMPLE_STEPS)
+        cpu = {"value": r["shots_per_s"], "unit": "shots/s", "cores": procs, "kind": "port",
+               "host_cores": host_cores(), "processes": procs,
+               "sample": f"{procs} processes x one config-2 shot sample each ({CPU_SAMPLE_STEPS} forward + "
+                         f"{CPU_SAMPLE_STEPS} backward steps of the C++ restatement on the migration model), "
+                         f"extrapolated to nt={NT}; {r['sec_per_shot']:.0f} s/shot"}
 
     if rank == 0:
         gcell = world * args.steps * 2 * (NT - 1) * g["n_pad"] / (ms_max / 1e3) / 1e9
@@ -510,12 +728,13 @@ def run_gpu(args):
                 "kernel": {"fwd_us_per_step": fwd_us, "bwd_us_per_step": bwd_us, "fwd_bytes": fwd_b,
                            "bwd_bytes": bwd_b},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "kernel": f"step_kernel<{dom}>",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": f"pair_kernel<{dom}> (two steps per launch)",
                              "peak_kind": peak_kind},
                 "gpu_launches": int(st["launches"]),
                 "clocks": clk.summary(),
                 "e2e": e2e,
                 "forms": forms,
+                "configs": configs,
                 "conditioning": conditioning,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
@@ -533,7 +752,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--forms", default="all",
                     help="other engine forms to time after the drop-in: all, none or a comma list of " +
-                         ", ".join(f[0] for f in FORMS))
+                         ", ".join(f["name"] for f in FORMS))
+    ap.add_argument("--configs", default="all",
+                    help="other benchmark configurations to time: all, none or a comma list of config1, config4, "
+                         "config5")
     ap.add_argument("--nt", type=int, default=None,
                     help="override the record length (small cases for ncu captures only; not a bench value)")
     args = ap.parse_args()
