@@ -270,6 +270,26 @@ int psdm_model_shot_noalloc(
     int32_t ny, int32_t nx, int32_t nx_w, const float* d_Vp_w, float dd_space, int32_t nt,
     float* d_Data_synth, void* stream);
 
+/*
+ * FP64 build of one shot of the mixed-precision form's schedule on the GPU:
+ * the error reference of the FP32 and FP16/BF16 forms (no counterpart in the
+ * reference, whose solvers are FP32).  The same per-cell update as the FP32
+ * kernels in double precision (FD coefficients, C-PML profiles and c2 set up
+ * in double from the FP32 inputs), snapshots every store_snap forward steps
+ * kept in FP64, imaging at the paired backward steps (for store_snap 1 the
+ * reference's pairing, solver_ac_backward_ram.f90:455-470).  Host arrays in
+ * the layouts of psdm_rtm_shot; PSDM_w (ny, nx_w) and, if not NULL,
+ * Fields_out (ny, nx_w, (nt_prop2-1)/store_snap) receive doubles.  Runs on
+ * `device` with its own device allocations, one launch per step; meant for
+ * accuracy checks, not speed.
+ */
+int psdm_rtm_shot_fp64(
+    int32_t device, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
+    const int32_t* nxRec, const int32_t* nyRec, const float* Data_source, const float* Data_target,
+    float dd, float dt, int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w, float added_space,
+    int32_t store_snap, int32_t nt_prop2, int32_t nt_taper, int32_t taper_option, int32_t N_taper,
+    int32_t N_zeros, double* PSDM_w, double* Fields_out);
+
 /* ---- host helpers: the reference's set-up arithmetic, same FP32 order ---- */
 
 /* finite_difference_coef (src/solver_FD_coeffs.f90:1-73); coef[acc+1]. */

@@ -22,7 +22,7 @@ EXPORTS = [
     "psdm_engine_reset_stats", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
-    "psdm_model_shot_noalloc", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
+    "psdm_model_shot_noalloc", "psdm_rtm_shot_fp64", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
     "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
     "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch", "psdm_engine_set_steps_per_launch",
     "psdm_freq_filter", "psdm_freq_filter_device", "psdm_butterworth_response",
@@ -63,6 +63,7 @@ _lib = None
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _I, _F, _P = C.c_int32, C.c_float, C.c_void_p
 
 
@@ -96,6 +97,8 @@ def lib():
     L.psdm_rtm_shot_device.argtypes = [
         _P, PP, _I, _I, _I, _i32p, _i32p, _P, _P, _F, _F, _I, _I, _I, _P, _F, _I, _I, _I, _I, _I, _I, _I, _P]
     L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
+    L.psdm_rtm_shot_fp64.argtypes = [_I, PP, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F,
+                                     _I, _I, _I, _I, _I, _I, _f64p, _P]
     L.psdm_model_shot_noalloc.argtypes = [PP, _I, _I, _I, _i32p, _i32p, _P, _F, _F, _I, _I, _I, _P, _F, _I, _P, _P]
     L.psdm_rtm_batch.argtypes = [_P, PP, _I, C.POINTER(Shot), _f32p, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]
     L.psdm_rtm_batch_device.argtypes = [_P, PP, _I, C.POINTER(Shot), _P, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]

@@ -249,6 +249,24 @@ class Engine:
         return out
 
 
+def rtm_shot_fp64(device: int, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target, dd, dt,
+                  ny, nx, nx_w, Vp_w, added_space, store_snap, nt_prop2, nt_taper, taper_option=0, N_taper=1,
+                  N_zeros=0, want_fields=False):
+    """psdm_rtm_shot_fp64: the FP64 build of one shot on `device` (the error
+    reference of the FP32 and mixed forms).  Returns the image (nx_w, ny)
+    float64 and, if asked, the snapshots (nsnap, nx_w, ny) float64."""
+    nxRec = _i32(nxRec)
+    img = np.zeros((nx_w, ny), dtype=np.float64)
+    nsnap = (nt_prop2 - 1) // store_snap
+    F = np.zeros((max(nsnap, 1), nx_w, ny), dtype=np.float64) if want_fields else None
+    L.check(L.lib().psdm_rtm_shot_fp64(
+        device, C.byref(prm.c()), nxRec.size, int(nxSou), int(nySou), nxRec, _i32(nyRec),
+        _f32(Data_source).reshape(-1), _f32(Data_target).reshape(-1), dd, dt, ny, nx, nx_w, _f32(Vp_w), added_space,
+        store_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, img,
+        F.ctypes.data if F is not None else None))
+    return (img, F[:nsnap]) if want_fields else img
+
+
 # ---- host helpers (reference set-up arithmetic, run in the library) --------
 
 def fd_coef(num: int, acc: int = 3) -> np.ndarray:
