@@ -32,17 +32,20 @@ def _model(engine, c):
 
 
 def _both(engine, fn):
-    """fn() with one launch per pass, then with one launch per step, and the
-    engine's launch counts of each."""
+    """fn() with one launch per pass, then with one launch per time step, and
+    the engine's launch counts of each; the engine is left in its default
+    form (two steps per launch)."""
     out = []
     try:
         for on in (True, False):
             engine.set_pass_launch(on)
+            engine.set_steps_per_launch(1)
             engine.reset_stats()
             r = fn()
             out.append((r, engine.stats()["launches"]))
     finally:
         engine.set_pass_launch(_DEFAULT)
+        engine.set_steps_per_launch(2)
     return out
 
 
