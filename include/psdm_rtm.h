@@ -217,6 +217,45 @@ int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on);
  */
 int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps);
 
+/*
+ * Planning against an HBM budget (the role of the reference's rtm_strategy,
+ * optimization.f90:114-188, which picks RAM, disk or checkpoint strategies
+ * from the memory per rank).
+ */
+typedef struct psdm_plan {
+    int32_t steps_per_launch;     /* launch form chosen (1 or 2) */
+    int32_t slots;                /* shots in flight for the batched calls (1: one shot at a time) */
+    int32_t checkpoint_interval;  /* 0: all snapshots in HBM; K > 0: FP32 checkpoints every K steps */
+    int32_t fits;                 /* 1 if the plan fits the budget */
+    int64_t bytes_per_slot;       /* device bytes of one shot in flight under the plan */
+    int64_t budget_bytes;         /* the budget planned against */
+    float probe_us[2];            /* per-step device time measured with 1 and 2 steps per launch (0: not probed) */
+} psdm_plan;
+
+/*
+ * Memory plan of shots of a window ny x nx_w with nt_prop2 / nt_taper steps
+ * (host arithmetic only, no device needed): the device bytes of one shot in
+ * flight for the snapshot form that prm->precision selects; slots =
+ * min(max_slots, what fits in budget_bytes less a 1 GiB reserve); for FP32
+ * shots whose snapshots do not fit, the checkpoint interval K that
+ * minimises their memory (one shot at a time).  Returns PSDM_ERR_NOMEM, with
+ * the sizes in psdm_last_error(), when not even that fits.  The plan's
+ * steps_per_launch is 2 and probe_us zero.
+ */
+int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t nt_prop2, int32_t nt_taper,
+                     int32_t store_snap, int32_t NumRec, int64_t budget_bytes, int32_t max_slots, psdm_plan* out);
+/*
+ * psdm_plan_memory against budget_bytes (0: the device's free memory plus
+ * what the engine holds), then, if probe != 0, a timed probe of the launch
+ * form: a 40-step forward pass of the window with one and with two steps per
+ * launch; the faster is kept.  The plan is applied to the engine (steps per
+ * launch, checkpoint interval); pass plan->slots as max_slots to the batched
+ * calls.
+ */
+int psdm_engine_autotune(psdm_engine* e, const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t nt_prop2,
+                         int32_t nt_taper, int32_t store_snap, int32_t NumRec, int64_t budget_bytes,
+                         int32_t max_slots, int32_t probe, psdm_plan* out);
+
 /* Shots in flight at a time in the last batched call. */
 int32_t psdm_engine_batch_slots(const psdm_engine* e);
 

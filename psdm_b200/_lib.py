@@ -22,7 +22,7 @@ EXPORTS = [
     "psdm_engine_reset_stats", "psdm_dynamic_window_solver_forward_ram", "psdm_dynamic_window_solver_backward_ram",
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
-    "psdm_model_shot_noalloc", "psdm_rtm_shot_fp64", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
+    "psdm_model_shot_noalloc", "psdm_plan_memory", "psdm_engine_autotune", "psdm_rtm_shot_fp64", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
     "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
     "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch", "psdm_engine_set_steps_per_launch",
     "psdm_freq_filter", "psdm_freq_filter_device", "psdm_butterworth_response",
@@ -38,6 +38,13 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("fwd_steps", C.c_int64), ("bwd_steps", C.c_int64), ("shots", C.c_int64),
                 ("fwd_ms", C.c_double), ("bwd_ms", C.c_double)]
+
+
+class Plan(C.Structure):
+    """psdm_plan (include/psdm_rtm.h)."""
+    _fields_ = [("steps_per_launch", C.c_int32), ("slots", C.c_int32), ("checkpoint_interval", C.c_int32),
+                ("fits", C.c_int32), ("bytes_per_slot", C.c_int64), ("budget_bytes", C.c_int64),
+                ("probe_us", C.c_float * 2)]
 
 
 class Shot(C.Structure):
@@ -99,6 +106,8 @@ def lib():
     L.psdm_model_shot.argtypes = [_P, PP, _I, _I, _I, _i32p, _i32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F, _I, _f32p]
     L.psdm_rtm_shot_fp64.argtypes = [_I, PP, _I, _I, _I, _i32p, _i32p, _f32p, _f32p, _F, _F, _I, _I, _I, _f32p, _F,
                                      _I, _I, _I, _I, _I, _I, _f64p, _P]
+    L.psdm_plan_memory.argtypes = [PP, _I, _I, _I, _I, _I, _I, C.c_int64, _I, C.POINTER(Plan)]
+    L.psdm_engine_autotune.argtypes = [_P, PP, _I, _I, _I, _I, _I, _I, C.c_int64, _I, _I, C.POINTER(Plan)]
     L.psdm_model_shot_noalloc.argtypes = [PP, _I, _I, _I, _i32p, _i32p, _P, _F, _F, _I, _I, _I, _P, _F, _I, _P, _P]
     L.psdm_rtm_batch.argtypes = [_P, PP, _I, C.POINTER(Shot), _f32p, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]
     L.psdm_rtm_batch_device.argtypes = [_P, PP, _I, C.POINTER(Shot), _P, _F, _F, _I, _I, _F, _I, _I, _I, _I, _I]

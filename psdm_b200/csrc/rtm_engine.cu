@@ -1911,6 +1911,126 @@ int psdm_rtm_batch_device(psdm_engine* e, const psdm_params* prm, int32_t nshots
 
 int32_t psdm_engine_batch_slots(const psdm_engine* e) { return e ? e->batch_slots : 0; }
 
+int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t nt_prop2, int32_t nt_taper,
+                     int32_t store_snap, int32_t NumRec, int64_t budget_bytes, int32_t max_slots, psdm_plan* out) {
+    if (!prm || !out) return fail(PSDM_ERR_ARG, "null argument");
+    TRY(check_params(prm));
+    if (ny < 1 || nx_w < 1 || nt_prop2 < 2 || nt_taper < nt_prop2 || store_snap < 1 || NumRec < 0 ||
+        budget_bytes < 0)
+        return fail(PSDM_ERR_ARG, "need a non-empty window, 2 <= nt_prop2 <= nt_taper, store_snap >= 1");
+    std::memset(out, 0, sizeof(*out));
+    out->steps_per_launch = 2;
+    out->budget_bytes = budget_bytes;
+    const Grid g = make_grid(prm->dPML, ny, nx_w);
+    const double cells = (double)g.cells(), field = (double)g.field_cells();
+    const int nsnap = (nt_prop2 - 1) / store_snap;
+    const double reserve = (double)(int64_t(1) << 30);
+    const double avail = (double)budget_bytes - reserve;
+    // One shot in flight: 13 grids (four wavefield levels, c2, phi and chi
+    // at two levels each), the pitched image, the launch arguments of both
+    // passes and the model window and traces.
+    const double base = 13.0 * cells * 4 + field * 4 + (double)(nt_prop2 + nt_taper) / 2 * sizeof(PairArgs) +
+                        ((double)ny * nx_w + (double)NumRec * nt_taper + nt_prop2) * 4;
+    const int mslots = std::min(max_slots > 0 ? (int)max_slots : kMaxSlots, kMaxSlots);
+    if (prm->precision != PSDM_PREC_FP32) {
+        // 16-bit snapshots, four FP32 staging buffers and the Kahan compensation
+        const double per = base + (double)nsnap * field * 2 + 5.0 * field * 4;
+        out->bytes_per_slot = (int64_t)per;
+        const double n = avail > 0 ? std::floor(avail / per) : 0.0;
+        out->slots = (int)std::min<double>(n, mslots);
+        out->fits = out->slots >= 1;
+        if (!out->fits)
+            return fail(PSDM_ERR_NOMEM, "one mixed-precision shot needs %.2f GB, the budget leaves %.2f GB",
+                        per / 1e9, avail / 1e9);
+        return PSDM_OK;
+    }
+    const double all = base + (double)nsnap * field * 4;
+    if (all <= avail) {
+        out->bytes_per_slot = (int64_t)all;
+        out->slots = (int)std::min<double>(std::floor(avail / all), mslots);
+        out->fits = 1;
+        return PSDM_OK;
+    }
+    // Checkpoints every K steps: the state (8 grids and two history rows) at
+    // each segment start but the first, a K-slot snapshot buffer, and the
+    // recomputing shot's own grids; the memory is smallest near
+    // K = sqrt(steps * state / snapshot).
+    const int nsteps = nt_prop2 - 1;
+    const double state = (8.0 * cells + 2.0 * g.nxt) * 4;
+    auto mem = [&](int K) {
+        const int nseg = (nsteps + K - 1) / K;
+        return base + 13.0 * cells * 4 + (double)K * field * 4 + (double)(nseg - 1) * state;
+    };
+    int best = 1;
+    for (int K = 1; K <= nsteps; ++K)
+        if (mem(K) < mem(best)) best = K;
+    best = std::max(best, std::min(16, nsteps));  // at most one state copy per 16 steps
+    out->bytes_per_slot = (int64_t)mem(best);
+    if (mem(best) > avail)
+        return fail(PSDM_ERR_NOMEM, "one FP32 shot needs %.2f GB even with checkpoints every %d steps, the budget "
+                    "leaves %.2f GB", mem(best) / 1e9, best, avail / 1e9);
+    out->checkpoint_interval = best;
+    out->slots = 1;
+    out->fits = 1;
+    return PSDM_OK;
+}
+
+int psdm_engine_autotune(psdm_engine* e, const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t nt_prop2,
+                         int32_t nt_taper, int32_t store_snap, int32_t NumRec, int64_t budget_bytes,
+                         int32_t max_slots, int32_t probe, psdm_plan* out) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    if (budget_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        budget_bytes = (int64_t)fr + e->total();
+    }
+    TRY(psdm_plan_memory(prm, ny, nx_w, nt_prop2, nt_taper, store_snap, NumRec, budget_bytes, max_slots, out));
+    if (probe) {
+        // A 40-step forward pass of the window (2000 m/s, no snapshots) in
+        // each launch form, timed on the engine's stream after a warm-up.
+        psdm_params p1 = *prm;
+        p1.precision = PSDM_PREC_FP32;
+        const int nt = 41;
+        std::vector<float> vp((size_t)ny * nx_w, 2000.0f);
+        float* d_vp = nullptr;
+        float* d_S = nullptr;
+        TRY(e->get("probe_vp", vp.size(), &d_vp));
+        TRY(e->get("probe_S", (size_t)nt, &d_S));
+        CUDA_TRY(cudaMemcpyAsync(d_vp, vp.data(), vp.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaMemsetAsync(d_S, 0, nt * sizeof(float), e->stream));
+        const int spl0 = e->steps_per_launch;
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        CUDA_TRY(cudaEventCreate(&t0));
+        CUDA_TRY(cudaEventCreate(&t1));
+        int rc = PSDM_OK;
+        for (int spl = 1; spl <= 2 && rc == PSDM_OK; ++spl) {
+            e->steps_per_launch = spl;
+            Shot s;
+            rc = setup_shot(e, &p1, ny, nx_w, 10.f, 1e-3f, d_vp, &s, "_probe");
+            const int zs = s.g.dn + std::min(2, ny) - 1, xs = s.g.dn + nx_w / 2;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && rc == PSDM_OK; ++rep) {
+                if (rep == 1 && cudaEventRecord(t0, e->stream) != cudaSuccess) rc = PSDM_ERR_CUDA;
+                if (rc == PSDM_OK) rc = run_forward(e, s, nt, 1, d_S, zs, xs, nullptr, 0, 0, nullptr, nullptr);
+                if (rc == PSDM_OK && rep == 1 && cudaEventRecord(t1, e->stream) != cudaSuccess) rc = PSDM_ERR_CUDA;
+            }
+            if (rc == PSDM_OK && cudaEventSynchronize(t1) == cudaSuccess && cudaEventElapsedTime(&ms, t0, t1) ==
+                                                                                 cudaSuccess)
+                out->probe_us[spl - 1] = ms * 1e3f / (nt - 1);
+        }
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        e->steps_per_launch = spl0;
+        TRY(rc);
+        TRY(sync(e));
+        out->steps_per_launch = (out->probe_us[0] > 0.f && out->probe_us[0] < out->probe_us[1]) ? 1 : 2;
+    }
+    e->steps_per_launch = out->steps_per_launch;
+    e->ckpt_interval = out->checkpoint_interval;
+    return PSDM_OK;
+}
+
 int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on) {
     TRY(check_engine(e));
     e->use_pass = on != 0;

@@ -227,6 +227,14 @@ class Engine:
         """psdm_engine_set_steps_per_launch: 2 (default) time steps per kernel launch, or 1."""
         L.check(L.lib().psdm_engine_set_steps_per_launch(self._h, int(steps)))
 
+    def autotune(self, prm: Params, ny: int, nx_w: int, nt_prop2: int, nt_taper: int, store_snap: int, nrec: int,
+                 budget_bytes: int = 0, max_slots: int = 0, probe: bool = True) -> dict:
+        """psdm_engine_autotune: plan against the budget (0 = free device memory), probe the launch form, apply."""
+        p = L.Plan()
+        L.check(L.lib().psdm_engine_autotune(self._h, C.byref(prm.c()), ny, nx_w, nt_prop2, nt_taper, store_snap,
+                                             nrec, int(budget_bytes), max_slots, int(bool(probe)), C.byref(p)))
+        return _plan_dict(p)
+
     def set_checkpointing(self, interval: int):
         """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
         L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))
@@ -247,6 +255,21 @@ class Engine:
             self._h, C.byref(prm.c()), nxRec.size, int(nxSou), int(nySou), nxRec, _i32(nyRec),
             _f32(Data_source).reshape(-1), dd, dt, ny, nx, nx_w, _f32(Vp_w), dd_space, nt, out))
         return out
+
+
+def _plan_dict(p) -> dict:
+    return {"steps_per_launch": p.steps_per_launch, "slots": p.slots, "checkpoint_interval": p.checkpoint_interval,
+            "fits": bool(p.fits), "bytes_per_slot": p.bytes_per_slot, "budget_bytes": p.budget_bytes,
+            "probe_us": [float(p.probe_us[0]), float(p.probe_us[1])]}
+
+
+def plan_memory(prm: Params, ny: int, nx_w: int, nt_prop2: int, nt_taper: int, store_snap: int, nrec: int,
+                budget_bytes: int, max_slots: int = 0) -> dict:
+    """psdm_plan_memory: slots and checkpoint interval against an HBM budget (host arithmetic only)."""
+    p = L.Plan()
+    L.check(L.lib().psdm_plan_memory(C.byref(prm.c()), ny, nx_w, nt_prop2, nt_taper, store_snap, nrec,
+                                     int(budget_bytes), max_slots, C.byref(p)))
+    return _plan_dict(p)
 
 
 def rtm_shot_fp64(device: int, prm: Params, nxSou: int, nySou: int, nxRec, nyRec, Data_source, Data_target, dd, dt,
