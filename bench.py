@@ -246,7 +246,7 @@ def run_reference(args):
 # binary16 / bfloat16 snapshots every ks steps; ckpt = checkpoint interval of
 # FP32 shots; spl = time steps per kernel launch.
 FORMS = [
-    dict(name="fp32_one_step", precision=0, ks=1, slots=0, spl=1),
+    dict(name="fp32_two_steps", precision=0, ks=1, slots=0, spl=2),
     dict(name="fp16_ks4", precision=1, ks=4, slots=0),
     dict(name="batch_fp16_ks4", precision=1, ks=4, slots=8),
     dict(name="batch_bf16_ks4", precision=2, ks=4, slots=8),
@@ -339,7 +339,7 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         ckpt = f.get("ckpt", 0)
         n = 2 * slots if slots else 4
         engine.set_checkpointing(ckpt)
-        engine.set_steps_per_launch(f.get("spl", 2))
+        engine.set_steps_per_launch(f.get("spl", 1))
         sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
 
         def run(k):
@@ -363,14 +363,14 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         engine.set_checkpointing(0)
-        engine.set_steps_per_launch(2)
+        engine.set_steps_per_launch(1)
         v = n / (e0.elapsed_time(e1) / 1e3)
         out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
                      "slots": engine.batch_slots() if slots else 1, "precision": ["f32", "fp16", "bf16"][precision],
                      "store_snap": ks}
         if ckpt:
             out[name]["checkpoint_interval"] = ckpt
-        if f.get("spl", 2) != 2:
+        if f.get("spl", 1) != 1:
             out[name]["steps_per_launch"] = f["spl"]
     return out
 
@@ -728,7 +728,7 @@ def run_gpu(args):
                 "kernel": {"fwd_us_per_step": fwd_us, "bwd_us_per_step": bwd_us, "fwd_bytes": fwd_b,
                            "bwd_bytes": bwd_b},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "kernel": f"pair_kernel<{dom}> (two steps per launch)",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": f"step_kernel<{dom}>",
                              "peak_kind": peak_kind},
                 "gpu_launches": int(st["launches"]),
                 "clocks": clk.summary(),

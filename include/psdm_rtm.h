@@ -197,6 +197,19 @@ int psdm_rtm_batch_device(
  */
 int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval);
 /*
+ * Boundary-saved reconstruction for FP32 shots (psdm_rtm_shot,
+ * psdm_rtm_shot_device) with store_snap 1: 1 saves
+ * the 3 C-PML cells next to the interior on each side at every forward step
+ * (4 B x (6 ny + 6 nx_w) per step) and rebuilds the source wavefield
+ * backwards in time on the interior during the backward pass, in place of
+ * holding nt_prop2 snapshots (the role of the reference's disk strategy,
+ * solver_ac_forward_disk.f90:469-517).  The image equals the plain shot's
+ * to rounding level (the reverse recursion is not bit-exact).  Its passes
+ * run two steps per launch.  0 (default) = off; takes precedence over
+ * checkpointing.
+ */
+int psdm_engine_set_reconstruction(psdm_engine* e, int32_t on);
+/*
  * Launch form of one shot's passes (psdm_rtm_shot, psdm_model_shot and their
  * device variants): 1 runs a pass whose steps allow it as one cooperative
  * launch in which each tile advances as soon as its neighbours finished the
@@ -208,12 +221,14 @@ int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on);
 /*
  * Time steps per kernel launch for every pass of the engine (no reference
  * counterpart; the reference advances its arrays one step at a time,
- * solver_ac_forward_ram.f90:344-573): 2 (default) advances each tile two
- * steps per launch, level n+1 computed on the tile and a 3-cell ring in
- * shared memory, so that the wavefield crosses HBM and the launch queue half
- * as often; 1 launches one kernel per step.  Same results bit for bit.  The
- * cooperative pass launch (psdm_engine_set_pass_launch) and checkpointed
- * shots use one step per launch.
+ * solver_ac_forward_ram.f90:344-573): 1 (default) launches one kernel per
+ * step; 2 advances each tile two steps per launch, level n+1 computed on the
+ * tile and a 3-cell ring in shared memory, so that the wavefield crosses HBM
+ * and the launch queue half as often.  Same results bit for bit.  On the
+ * B200 the one-step form is currently the faster (see psdm_engine_autotune,
+ * which times both).  The cooperative pass launch
+ * (psdm_engine_set_pass_launch) and checkpointed shots use one step per
+ * launch; reconstruction (psdm_engine_set_reconstruction) uses two.
  */
 int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps);
 
@@ -240,7 +255,7 @@ typedef struct psdm_plan {
  * shots whose snapshots do not fit, the checkpoint interval K that
  * minimises their memory (one shot at a time).  Returns PSDM_ERR_NOMEM, with
  * the sizes in psdm_last_error(), when not even that fits.  The plan's
- * steps_per_launch is 2 and probe_us zero.
+ * steps_per_launch is 1 and probe_us zero.
  */
 int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t nt_prop2, int32_t nt_taper,
                      int32_t store_snap, int32_t NumRec, int64_t budget_bytes, int32_t max_slots, psdm_plan* out);

@@ -24,7 +24,7 @@ EXPORTS = [
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
     "psdm_model_shot_noalloc", "psdm_plan_memory", "psdm_engine_autotune", "psdm_rtm_shot_fp64", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
     "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
-    "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch", "psdm_engine_set_steps_per_launch",
+    "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch", "psdm_engine_set_steps_per_launch", "psdm_engine_set_reconstruction",
     "psdm_freq_filter", "psdm_freq_filter_device", "psdm_butterworth_response",
     "psdm_nav_read", "psdm_channel_positions", "psdm_geometry_mcs", "psdm_linear_2d", "psdm_batmodel_from_velocity",
     "psdm_nav_read_was", "psdm_nav_read_obs", "psdm_geometry_was", "psdm_bathymetry_nav", "psdm_relocate_obs",
@@ -117,6 +117,7 @@ def lib():
     L.psdm_engine_set_checkpointing.argtypes = [_P, _I]
     L.psdm_engine_set_pass_launch.argtypes = [_P, _I]
     L.psdm_engine_set_steps_per_launch.argtypes = [_P, _I]
+    L.psdm_engine_set_reconstruction.argtypes = [_P, _I]
     L.psdm_freq_filter.argtypes = [_P, _f32p, _I, _F, _I, _I, _F, _F]
     L.psdm_freq_filter_device.argtypes = [_P, _P, _I, _F, _I, _I, _F, _F]
     L.psdm_su_write_image.argtypes = [C.c_char_p, _I, _I, _F, _F, _I, _f32p, _I]

@@ -82,9 +82,10 @@ struct psdm_engine {
         cudaGraphExec_t exec = nullptr;
     } graphs[3];
     bool use_graphs = true;
-    // Time steps per launch: 2 = pair launches (rtm_pair.cu), 1 = one launch
-    // per step.  Captured pair loops, one per pass kind.
-    int steps_per_launch = 2;
+    // Time steps per launch: 1 (default, the faster form on the B200) = one
+    // launch per step, 2 = pair launches (rtm_pair.cu).  Captured pair loops,
+    // one per pass kind.
+    int steps_per_launch = 1;
     struct PairGraphCache {
         std::vector<PairArgs> args;
         cudaGraphExec_t exec = nullptr;
@@ -97,6 +98,7 @@ struct psdm_engine {
     cudaEvent_t pass_staged[3] = {nullptr, nullptr, nullptr};  // copies out of the staging buffers done
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
+    bool recon = false;     // FP32 shots reconstruct the source wavefield from a saved band
     std::map<std::pair<int, int>, std::array<int, 2>> fft_plans;  // (length, batch) -> cuFFT plans
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
     std::map<float, std::pair<int, std::vector<float>>> div_cache;
@@ -650,9 +652,11 @@ void pair_rot_advance(PairRot& r, int nsub) {
 // snapshot slots staged by the last launch (to be converted after the pass).
 int make_pairs(psdm_engine* e, const Shot& s, int mode, const std::vector<StepArgs>& steps, size_t first,
                size_t count, const std::vector<int>& row_slot, int nrec, const int* h_rec_cell, const MixedBufs* mb,
-               const std::string& tag, std::vector<PairArgs>* out, float** last, std::vector<int>* pending) {
+               const std::string& tag, std::vector<PairArgs>* out, float** last, std::vector<int>* pending,
+               float** prev_last = nullptr) {
     PairRot r = pair_rot_start(s);
     *last = r.cur;
+    if (prev_last) *prev_last = r.prev;
     if (pending) pending->clear();
     if (count == 0) return PSDM_OK;
     PairArgs base;
@@ -744,6 +748,7 @@ int make_pairs(psdm_engine* e, const Shot& s, int mode, const std::vector<StepAr
         i += ns;
     }
     *last = r.cur;
+    if (prev_last) *prev_last = r.prev;
     if (pending) *pending = pend;
     return PSDM_OK;
 }
@@ -1218,6 +1223,110 @@ int rtm_shot_checkpointed(psdm_engine* e, const psdm_params* prm, int NumRec, in
     return PSDM_OK;
 }
 
+// ---- boundary-saved reconstruction of the source wavefield -----------------
+//
+// In place of keeping the forward pass's snapshots (the RAM strategy) or
+// writing them to files (the disk strategy, solver_ac_forward_disk.f90:
+// 469-517), the forward pass (two steps per launch) saves every level's band
+// -- the 3 C-PML cells next to the interior on each side -- and keeps its
+// last two levels; the backward pass runs the source wavefield backwards in
+// time on the interior, P(L) = (2 P(L+1) + c2 (...)) - P(L+2) with the band
+// of level L put back, which yields each imaging step's snapshot just before
+// the step needs it.  The reverse recursion repeats the forward step's
+// rounding in the opposite direction, so the image equals the plain shot's
+// to rounding level, not bit for bit.  Memory: the band, 4 B x (6 ny + 6 nx)
+// per step, in place of ny x nx_w per step.  FP32 with store_snap 1; the
+// passes use pair launches (the band is written by the pair kernels' tiles)
+// whatever the engine's launch form.
+int rtm_shot_reconstructed(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou,
+                           const int* nxRec, const int* nyRec, const float* d_S, const float* d_tgt, float dd,
+                           float dt, int ny, int nx, int nx_w, const float* d_vp, float added_space, int nt_prop2,
+                           int nt_taper, const float* wts, float* d_img) {
+    Shot f, b;  // forward (its last two levels feed the reconstruction) and backward states
+    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &f, "_rcf"));
+    TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &b));
+    WinGeom w;
+    TRY(window_geometry(f.g, NumRec, nxSou, nySou, nxRec, nyRec, dd, nx, added_space, &w));
+    if (w.nx_w_calc != nx_w)
+        return fail(PSDM_ERR_ARG, "nx_w=%d does not match the window of this geometry (%d)", nx_w, w.nx_w_calc);
+    const size_t fstride = f.g.field_cells();
+    const int nsnap = nt_prop2 - 1;
+    const size_t nband = (size_t)band_count(ny, nx_w);
+    float *band = nullptr, *snap = nullptr, *d_imgp = nullptr;
+    TRY(e->get("rc_band", nband * (size_t)(nt_prop2 + 1), &band));
+    TRY(e->get("rc_snap", 2 * fstride, &snap));
+    TRY(e->get("image_pitched", fstride, &d_imgp));
+    CUDA_TRY(cudaMemsetAsync(band, 0, nband * (nt_prop2 + 1) * sizeof(float), e->stream));
+    TRY(e->record(0));
+    // forward: no snapshots, the band of every level k (written by step k)
+    std::vector<StepArgs> fwd;
+    std::vector<int> frow;
+    TRY(build_forward(e, f, nt_prop2, 1, d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, "_rcf", &fwd, false,
+                      &frow));
+    std::vector<PairArgs> fp;
+    float *last = nullptr, *prev = nullptr;
+    TRY(make_pairs(e, f, 0, fwd, 0, fwd.size(), frow, 0, nullptr, nullptr, "_rcf", &fp, &last, nullptr, &prev));
+    for (size_t q = 0, i = 0; q < fp.size(); i += fp[q].nsub, ++q)
+        for (int j = 0; j < fp[q].nsub; ++j) fp[q].sub[j].band = band + nband * (size_t)(i + j + 2);
+    TRY(launch_pairs(e, 0, fp));
+    e->fwd_steps += nt_prop2 - 1;
+    TRY(e->record(1));
+    // backward: slot m is imaged at step k = nt_taper + 1 - m from a
+    // snapshot the reverse step writes just before the launch
+    CUDA_TRY(cudaMemsetAsync(d_imgp, 0, fstride * sizeof(float), e->stream));
+    std::vector<StepArgs> bwd;
+    std::vector<int> brow, slot;
+    TRY(build_backward(e, b, nt_taper, 1, nt_taper, d_tgt, 1, NumRec, w.zr.data(), w.xr.data(), snap, 1, nsnap, wts,
+                       d_imgp, "", &bwd, &slot, false, &brow));
+    std::vector<PairArgs> bp;
+    float* blast = nullptr;
+    TRY(make_pairs(e, b, 1, bwd, 0, bwd.size(), brow, 0, nullptr, nullptr, "", &bp, &blast, nullptr));
+    const StepArgs& fa = fwd[0];
+    ReconArgs r;
+    std::memset(&r, 0, sizeof(r));
+    r.c2 = f.c2;
+    for (int k = 0; k < 4; ++k) r.cf2[k] = f.cf2[k];
+    r.nyt = f.g.nyt; r.nxt = f.g.nxt; r.ldz = f.g.ldz; r.ny = ny; r.nx = nx_w; r.dn = f.g.dn; r.zoff = f.g.zoff;
+    r.ldf = f.g.ldf;
+    r.fs = f.fs;
+    r.row_slot = fa.row_slot;
+    r.inj_cols = fa.inj_cols;
+    r.inj_trace = d_S;
+    r.dt = f.dt; r.inv_dt = f.inv_dt; r.div_lo = f.div_lo; r.div_hi = f.div_hi; r.div_tiny = f.div_tiny;
+    r.fast_div = f.fast_div;
+    float* cur = prev;  // level m = nsnap
+    float* nxt = last;  // level m + 1
+    int m_next = nsnap;  // the next slot the recursion produces
+    for (size_t q = 0, i = 0; q < bp.size(); i += bp[q].nsub, ++q) {
+        for (int j = 0; j < bp[q].nsub; ++j) {
+            const int m = slot[i + j] > 0 ? slot[i + j] : 0;
+            bp[q].sub[j].field = nullptr;
+            if (m <= 0) continue;
+            while (m_next >= m) {  // P(m_next - 1) from P(m_next), P(m_next + 1); its snapshot is slot m_next
+                r.pc = cur;
+                r.pn = nxt;
+                r.band_L = band + nband * (size_t)(m_next - 1);
+                r.snap = snap + (size_t)j * fstride;
+                r.inj_t = m_next - 1;  // the source sample of forward step m_next + 1
+                const int rc = launch_reconstruct(r, e->stream);
+                if (rc) return fail(PSDM_ERR_CUDA, "reconstruction launch: %s", cudaGetErrorString((cudaError_t)rc));
+                e->launches += 2;
+                std::swap(cur, nxt);  // now cur = level m_next - 1, nxt = level m_next
+                --m_next;
+            }
+            bp[q].sub[j].field = snap + (size_t)j * fstride;
+        }
+        const int rc = launch_pair(1, bp[q], e->stream);
+        if (rc) return fail(PSDM_ERR_CUDA, "pair launch: %s", cudaGetErrorString((cudaError_t)rc));
+        e->launches += 1;
+    }
+    e->bwd_steps += (int64_t)bwd.size();
+    TRY(e->record(2));
+    CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)b.g.ldf * sizeof(float),
+                               (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
+    return PSDM_OK;
+}
+
 // One shot of RTM with every array in device memory
 // (calculate_PSDM_RTM.f90:395-466).  Asynchronous on e->stream.
 int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
@@ -1287,6 +1396,12 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
         CUDA_TRY(cudaMemcpy2DAsync(d_img, (size_t)ny * sizeof(float), d_imgp, (size_t)s.g.ldf * sizeof(float),
                                    (size_t)ny * sizeof(float), nx_w, cudaMemcpyDeviceToDevice, e->stream));
         return PSDM_OK;
+    }
+    if (e->recon) {
+        if (store_snap != 1) return fail(PSDM_ERR_ARG, "reconstruction of the source wavefield needs store_snap 1");
+        const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, taper_option, N_taper, N_zeros);
+        return rtm_shot_reconstructed(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_S, d_tgt, dd, dt, ny, nx, nx_w,
+                                      d_vp, added_space, nt_prop2, nt_taper, wts.data(), d_img);
     }
     if (e->ckpt_interval > 0) {
         const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, taper_option, N_taper, N_zeros);
@@ -1919,7 +2034,7 @@ int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t n
         budget_bytes < 0)
         return fail(PSDM_ERR_ARG, "need a non-empty window, 2 <= nt_prop2 <= nt_taper, store_snap >= 1");
     std::memset(out, 0, sizeof(*out));
-    out->steps_per_launch = 2;
+    out->steps_per_launch = 1;
     out->budget_bytes = budget_bytes;
     const Grid g = make_grid(prm->dPML, ny, nx_w);
     const double cells = (double)g.cells(), field = (double)g.field_cells();
@@ -2042,6 +2157,13 @@ int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps) {
     if (steps != 1 && steps != 2) return fail(PSDM_ERR_ARG, "steps per launch must be 1 or 2 (got %d)", steps);
     TRY(sync(e));
     e->steps_per_launch = steps;
+    return PSDM_OK;
+}
+
+int psdm_engine_set_reconstruction(psdm_engine* e, int32_t on) {
+    TRY(check_engine(e));
+    TRY(sync(e));
+    e->recon = on != 0;
     return PSDM_OK;
 }
 

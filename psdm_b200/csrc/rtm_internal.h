@@ -175,7 +175,38 @@ struct SubStep {
     int inj_t;                  // injection sample index of this step
     int rec_t;                  // forward: receiver sample taken from this sub-step's level, or -1
     int pad_;
+    float* band;                // forward: this level's band (band_index) written, or null
 };
+
+// The band of a padded grid: the 3 C-PML cells next to the interior on each
+// side (x strips over the interior rows, z strips over the interior
+// columns), nband = 6*ny + 6*nx values, at index
+//   x strips: col * ny + (z - dn), col 0..2 left (x = dn-3..dn-1), 3..5 right;
+//   z strips: 6*ny + (x - dn) * 6 + row, row 0..2 bottom, 3..5 top.
+// With it every interior cell's stencil has its operands: the interior and
+// the band.
+inline int band_count(int ny, int nx) { return 6 * ny + 6 * nx; }
+
+// Reverse time step of the interior (boundary-saved reconstruction of the
+// source wavefield): pn = level L+2 in, level L out, pc = level L+1
+// (interior and band filled).  snap = (P(L+2) - P(L)) * 0.5 / dt on the
+// interior; band_L = the saved band of level L, written into pn's band.
+struct ReconArgs {
+    const float* pc;
+    float* pn;
+    const float* c2;
+    const float* band_L;
+    float* snap;
+    float cf2[4];
+    int nyt, nxt, ldz, ny, nx, dn, zoff, ldf, fs;
+    const int* row_slot;
+    const int* inj_cols;
+    const float* inj_trace;
+    int inj_t;
+    float dt, inv_dt, div_lo, div_hi, div_tiny;
+    int fast_div;
+};
+int launch_reconstruct(const ReconArgs& r, void* stream);
 
 constexpr int kPairRects = 48;
 

@@ -28,10 +28,11 @@
 // rows x 28 columns, level n staged in shared memory by bulk asynchronous
 // copies, each thread sliding a float4 x 7-column window through registers
 // with the packed FP32x2 stencil of the one-step interior tiles; and
-// "generic" tiles (rect type 1, at most 32 x 32 cells) for everything else:
+// "generic" tiles (rect type 1, at most 26 x 32 cells) for everything else:
 // C-PML strips and corners (with the phi/chi recursions of
 // src/solver_PML_matrices.f90:1-111), the free-surface and injection rows,
-// and the interior cells next to them, one cell per thread at a time.
+// and the interior cells next to them: a lane per row, a warp per run of
+// columns, one cell per thread at a time.
 //
 // Reach: a cell's update reads its neighbours within 3 cells, except where
 // a stencil centre is clamped (the reference copies the derivative at
@@ -69,8 +70,9 @@ constexpr int HS1 = TZC + 8;        // rows of the level n+1 tile (3-row ring ro
 constexpr int Q0 = HS0 / 4, Q1 = HS1 / 4;
 constexpr int WS0 = TXC + 12, WS1 = TXC + 6;
 constexpr int kCleanFloats = HS0 * WS0 + HS1 * WS1;
-// Generic tiles: at most GZ x GX cells.
-constexpr int GZ = 32, GX = 32;
+// Generic tiles: at most GZ x GX cells; GZ + 6 = 32 rows, one per lane, in
+// the first step.
+constexpr int GZ = 26, GX = 32;
 constexpr int GH0 = GZ + 12, GW0 = GX + 12;  // level n on the tile + 6
 constexpr int GH1 = GZ + 6, GW1 = GX + 6;    // level n+1, phi and chi at n+1 on the tile + 3
 constexpr int kGenericFloats = GH0 * GW0 + 5 * GH1 * GW1 + GW1;
@@ -199,7 +201,11 @@ __device__ __forceinline__ void clean_phase(const PairArgs& P, float* S0, float*
     const int nq = PH == 0 ? (nrows >> 2) + 2 : (nrows >> 2);
     const int ncl = PH == 0 ? ncols + 6 : ncols;
     const int cb = (w * ncl) >> 2, ce = ((w + 1) * ncl) >> 2;
-    if (lane >= nq || cb >= ce) return;
+    // at most (TXC + 6) / 4 columns per warp: the loop below is unrolled to
+    // that bound, so the register window shifts by renaming
+    constexpr int MAXC = PH == 0 ? (TXC + 6 + NWARP - 1) / NWARP : XSC;
+    const int ncw = ce - cb;
+    if (lane >= nq || ncw <= 0) return;
     const int zd = PH == 0 ? z0 - 4 + 4 * lane : z0 + 4 * lane;
     constexpr int SQ = PH == 0 ? Q0 : Q1;
     const float4* __restrict__ src = reinterpret_cast<const float4*>(PH == 0 ? S0 : S1);
@@ -217,7 +223,7 @@ __device__ __forceinline__ void clean_phase(const PairArgs& P, float* S0, float*
     float amax_t = 0.f;
     int g = (xb + cb) * a.ldz + zd;
     int fi = (xb + cb - dn) * a.ldf + (zd - a.zoff - dn);
-    float4 pmN = PH == 0 ? *reinterpret_cast<const float4*>(a.pm + g) : S0v[(cb + 6) * Q0 + lane + 2];
+    float4 pmN = PH == 0 ? __ldg(reinterpret_cast<const float4*>(a.pm + g)) : S0v[(cb + 6) * Q0 + lane + 2];
     float4 c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
     float4 Fn = make_float4(0.f, 0.f, 0.f, 0.f), In = Fn, Cn = Fn;
     uint2 Fr = make_uint2(0u, 0u);
@@ -235,20 +241,22 @@ __device__ __forceinline__ void clean_phase(const PairArgs& P, float* S0, float*
     float4 win[7];
 #pragma unroll
     for (int k = 0; k < 6; ++k) win[k] = src[(cb + k) * SQ + sr];
-#pragma unroll 1
-    for (int c = cb; c < ce; ++c) {
+#pragma unroll
+    for (int j = 0; j < MAXC; ++j) {
+        if (j >= ncw) break;
+        const int c = cb + j;
         win[6] = src[(c + 6) * SQ + sr];
         const float4 zm = src[(c + 3) * SQ + sr - 1];
         const float4 zp = src[(c + 3) * SQ + sr + 1];
         const float4 pmv = pmN, c2v = c2N;
-        if (c + 1 < ce) {
-            pmN = PH == 0 ? *reinterpret_cast<const float4*>(a.pm + g + a.ldz) : S0v[(c + 7) * Q0 + lane + 2];
+        if (j + 1 < ncw) {
+            pmN = PH == 0 ? __ldg(reinterpret_cast<const float4*>(a.pm + g + a.ldz)) : S0v[(c + 7) * Q0 + lane + 2];
             c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g + a.ldz));
         }
         const float4 Fc = Fn, Ic = In, Cc = Cn;
         const uint2 Frc = Fr;
         const bool t = rowT && c >= tc0 && c < tc1;
-        if (c + 1 < ce && rowT && c + 1 >= tc0 && c + 1 < tc1) {
+        if (j + 1 < ncw && rowT && c + 1 >= tc0 && c + 1 < tc1) {
             if (img) {
                 Fn = __ldg(reinterpret_cast<const float4*>(s.field + fi + a.ldf));
                 In = *reinterpret_cast<const float4*>(a.image + fi + a.ldf);
@@ -388,16 +396,18 @@ __device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, i
     const float d2y = D2(AZ, a.cf2);
     const int g = x * a.ldz + zd;
     const float pc = SS[(x - ox) * SP + (zd - oz)];
-    const float pmo = SUB == 0 ? a.pm[g] : G.S0[i0];
+    // Every HBM operand of a pair launch is only read during the launch
+    // (its outputs go to other buffers), so read-only cached loads are safe.
+    const float pmo = SUB == 0 ? __ldg(a.pm + g) : G.S0[i0];
     const float c2v = __ldg(a.c2 + g);
     float pp = pc, ppm = pmo;
     if (side) {
         if (SUB == 0) {
-            pp = a.side_p[x];
-            ppm = a.side_pm[x];
+            pp = __ldg(a.side_p + x);
+            ppm = __ldg(a.side_pm + x);
         } else {
             pp = G.SD1[x - (G.x0 - 3)];
-            ppm = a.side_p[x];
+            ppm = __ldg(a.side_p + x);
         }
     }
     const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
@@ -413,11 +423,11 @@ __device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, i
             float dph, phold, chold;
             if (SUB == 0) {
                 const float* ph = a.phix_in + (size_t)ci * a.ldz + zd;
-#define PX(k) ph[(k) * a.ldz]
+#define PX(k) __ldg(ph + (k) * a.ldz)
                 dph = D1(PX, a.cf1);
 #undef PX
-                phold = a.phix_in[g];
-                chold = P.chix_in[g];
+                phold = __ldg(a.phix_in + g);
+                chold = __ldg(P.chix_in + g);
             } else {
                 const float* ph = G.F1x + (ci - (G.x0 - 3)) * GH1 + (zd - (G.z0 - 3));
 #define PX(k) ph[(k) * GH1]
@@ -448,11 +458,11 @@ __device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, i
             float dph, phold, chold;
             if (SUB == 0) {
                 const float* ph = a.phiz_in + (size_t)x * a.ldz + cj;
-#define PZ(k) ph[(k)]
+#define PZ(k) __ldg(ph + (k))
                 dph = D1(PZ, a.cf1);
 #undef PZ
-                phold = a.phiz_in[g];
-                chold = P.chiz_in[g];
+                phold = __ldg(a.phiz_in + g);
+                chold = __ldg(P.chiz_in + g);
             } else {
                 const float* ph = G.F1z + (x - (G.x0 - 3)) * GH1 + (cj - (G.z0 - 3));
 #define PZ(k) ph[(k)]
@@ -506,6 +516,12 @@ __device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, i
         G.S0[i0] = out;
         if (side) P.side_out[1][x] = p3;
     }
+    if (MODE == 0 && inT && s.band != nullptr) {  // the band of this level (boundary-saved reconstruction)
+        if (kz == 0 && kx >= 1 && kx <= 3)
+            s.band[(x < dn ? x - (dn - 3) : 3 + x - (dn + a.nx)) * a.ny + (z - dn)] = out;
+        else if (kx == 0 && kz >= 1 && kz <= 3)
+            s.band[6 * a.ny + (x - dn) * 6 + (z >= dn + a.ny ? z - (dn + a.ny) : 3 + z - (dn - 3))] = out;
+    }
     if (inT && kx == 0 && kz == 0) {
         const int fi = (x - dn) * a.ldf + (z - dn);
         if (MODE == 0) {
@@ -547,7 +563,6 @@ __host__ __device__ __forceinline__ void generic_bounds(const PairArgs& P, int r
 template <int MODE>
 __device__ __forceinline__ void pair_generic_tile(const PairArgs& P, float* sm, int r, int t, int b) {
     const StepArgs& a = P.a;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
     GenTile G;
     generic_bounds(P, r, t, &G.z0, &G.z1, &G.x0, &G.x1);
     G.S0 = sm;
@@ -559,22 +574,32 @@ __device__ __forceinline__ void pair_generic_tile(const PairArgs& P, float* sm, 
     G.SD1 = G.X1z + GH1 * GW1;
     const int H = G.z1 - G.z0, W = G.x1 - G.x0;
     const int H0 = H + 12, W0 = W + 12;
-    for (int i = tid; i < H0 * W0; i += NT) {
-        const int xl = i / H0, zl = i - xl * H0;
-        const int zd = G.z0 - 6 + zl, x = G.x0 - 6 + xl;
-        G.S0[xl * GH0 + zl] = (zd >= 0 && zd < a.ldz && x >= 0 && x < a.nxt) ? a.p[(size_t)x * a.ldz + zd] : 0.f;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    for (int xl = w; xl < W0; xl += NWARP) {
+        const int x = G.x0 - 6 + xl;
+        const bool xin = x >= 0 && x < a.nxt;
+        for (int zl = lane; zl < H0; zl += 32) {
+            const int zd = G.z0 - 6 + zl;
+            G.S0[xl * GH0 + zl] = (xin && zd >= 0 && zd < a.ldz) ? __ldg(a.p + (size_t)x * a.ldz + zd) : 0.f;
+        }
     }
     __syncthreads();
+    // first step on rows [z0-3, z1+3) (a lane each) x columns [x0-3, x1+3)
+    // (a run of columns per warp)
     const int H1 = H + 6, W1 = W + 6;
-    for (int i = tid; i < H1 * W1; i += NT) {
-        const int xl = i / H1, zl = i - xl * H1;
-        pair_cell<MODE, 0>(P, G, G.z0 - 3 + zl, G.x0 - 3 + xl);
+    if (lane < H1) {
+        const int zd = G.z0 - 3 + lane;
+        const int cb = (w * W1) / NWARP, ce = ((w + 1) * W1) / NWARP;
+#pragma unroll 1
+        for (int c = cb; c < ce; ++c) pair_cell<MODE, 0>(P, G, zd, G.x0 - 3 + c);
     }
     if (P.nsub == 2) {
         __syncthreads();
-        for (int i = tid; i < H * W; i += NT) {
-            const int xl = i / H, zl = i - xl * H;
-            pair_cell<MODE, 1>(P, G, G.z0 + zl, G.x0 + xl);
+        if (lane < H) {
+            const int zd = G.z0 + lane;
+            const int cb = (w * W) / NWARP, ce = ((w + 1) * W) / NWARP;
+#pragma unroll 1
+            for (int c = cb; c < ce; ++c) pair_cell<MODE, 1>(P, G, zd, G.x0 + c);
         }
     }
     if (MODE == 0 && P.rec_first != nullptr)
@@ -701,6 +726,67 @@ __global__ void __launch_bounds__(NT, 5) pair_batch_kernel(const PairBatchParams
     }
 }
 
+// Reverse step of the interior: the forward update
+// P(L+2) = (-P(L) + 2 P(L+1)) + c2 ((d2x + d2y) + src) solved for P(L) with
+// the same c2 term, P(L) = (2 P(L+1) + c2 (...)) - P(L+2); the free-surface
+// row stays zero.  One thread per interior cell (rows fastest).
+__global__ void reconstruct_kernel(const ReconArgs r) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // interior row
+    const int i = blockIdx.y;                              // interior column
+    if (j >= r.ny || i >= r.nx) return;
+    const int z = r.dn + j, x = r.dn + i, zd = z + r.zoff;
+    const size_t g = (size_t)x * r.ldz + zd;
+    const float p2 = r.pn[g];
+    float out = 0.f;
+    if (!(r.fs && j == 0)) {
+        const float* colc = r.pc + g;
+#define AX(k) __ldg(colc + (ptrdiff_t)(k) * r.ldz)
+#define AZ(k) __ldg(colc + (k))
+        const float d2x = D2(AX, r.cf2);
+        const float d2y = D2(AZ, r.cf2);
+#undef AX
+#undef AZ
+        float src = 0.f;
+        if (r.row_slot != nullptr) {
+            const int rs = __ldg(r.row_slot + zd);
+            if (rs >= 0) {
+                const int t = __ldg(r.inj_cols + rs * r.nxt + x);
+                if (t >= 0) src = __ldg(r.inj_trace + r.inj_t);
+            }
+        }
+        const float b = __fmul_rn(__ldg(r.c2 + g), __fadd_rn(__fadd_rn(d2x, d2y), src));
+        out = __fsub_rn(__fadd_rn(__fmul_rn(2.f, __ldg(r.pc + g)), b), p2);
+    }
+    r.pn[g] = out;
+    StepArgs da;  // the division by dt of the snapshots
+    da.dt = r.dt;
+    da.inv_dt = r.inv_dt;
+    da.div_lo = r.div_lo;
+    da.div_hi = r.div_hi;
+    da.div_tiny = r.div_tiny;
+    da.fast_div = r.fast_div;
+    r.snap[(size_t)i * r.ldf + j] = div_dt(da, __fmul_rn(__fsub_rn(p2, out), 0.5f));
+}
+
+// The saved band of level L into its cells of pn.
+__global__ void band_fill_kernel(const ReconArgs r) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nxb = 6 * r.ny;
+    if (q >= nxb + 6 * r.nx) return;
+    int z, x;
+    if (q < nxb) {
+        const int col = q / r.ny, j = q - col * r.ny;
+        z = r.dn + j;
+        x = col < 3 ? r.dn - 3 + col : r.dn + r.nx + (col - 3);
+    } else {
+        const int u = q - nxb, i = u / 6, row = u - 6 * i;
+        x = r.dn + i;
+        z = row < 3 ? r.dn + r.ny + row : r.dn - 3 + (row - 3);
+        if (r.fs && z < r.dn) return;  // above a free surface: stays zero
+    }
+    r.pn[(size_t)x * r.ldz + z + r.zoff] = r.band_L[q];
+}
+
 constexpr int kPairSmemBytes = kPairFloats * (int)sizeof(float);
 
 template <int MODE>
@@ -760,6 +846,14 @@ int launch_pair(int mode, const PairArgs& P, void* stream) {
     if (mode == 0) return launch_persistent(pair_kernel<0>, P, tiles, sms * pair_blocks_per_sm<0>(), st);
     if (mode == 1) return launch_persistent(pair_kernel<1>, P, tiles, sms * pair_blocks_per_sm<1>(), st);
     return launch_persistent(pair_kernel<2>, P, tiles, sms * pair_blocks_per_sm<2>(), st);
+}
+
+int launch_reconstruct(const ReconArgs& r, void* stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    reconstruct_kernel<<<dim3((r.ny + 127) / 128, r.nx), 128, 0, st>>>(r);
+    const int nb = band_count(r.ny, r.nx);
+    band_fill_kernel<<<(nb + 255) / 256, 256, 0, st>>>(r);
+    return (int)cudaGetLastError();
 }
 
 int launch_pair_batch(const PairBatchParams& bp, int num_sms, void* stream) {

@@ -235,6 +235,10 @@ class Engine:
                                              nrec, int(budget_bytes), max_slots, int(bool(probe)), C.byref(p)))
         return _plan_dict(p)
 
+    def set_reconstruction(self, on: bool):
+        """psdm_engine_set_reconstruction: rebuild the source wavefield from a saved band (FP32, store_snap 1)."""
+        L.check(L.lib().psdm_engine_set_reconstruction(self._h, int(bool(on))))
+
     def set_checkpointing(self, interval: int):
         """psdm_engine_set_checkpointing: K > 0 keeps states every K steps instead of all snapshots."""
         L.check(L.lib().psdm_engine_set_checkpointing(self._h, int(interval)))

@@ -82,7 +82,7 @@ int main(int argc, char** argv) {
                     if (z < dn || z >= dn + ny || x < dn || x >= dn + nx || (fs && z == dn) || inj_row[z])
                         ++clean_err;
                 }
-        } else if (z1 - z0 > 32 || x1 - x0 > 32) {
+        } else if (z1 - z0 > 26 || x1 - x0 > 32) {
             ++shape_err;
         }
         // level-n cells a tile has: generic tile + 6; clean: the staged block

@@ -28,5 +28,5 @@ def test_autotune_probe_and_apply(engine, oracle):
                                nt_snap=c["nt"], nt_prop2=c["nt"], nt_taper=c["nt"])
         assert np.array_equal(img, want)
     finally:
-        engine.set_steps_per_launch(2)
+        engine.set_steps_per_launch(1)
         engine.set_checkpointing(0)

@@ -1,11 +1,11 @@
-"""Two time steps per launch (the default) against one launch per step, bit
+"""Two time steps per launch against one launch per step (the default), bit
 for bit, through the C ABI: snapshots and receiver traces of forward passes
 with an even and an odd number of steps, images of both statement orders
 with and without a free surface, tapers, store_snap > 1, colliding
 receivers, sources and receivers on the free-surface row or inside the
 interior, the mixed-precision form with one or two snapshots per launch,
 and batched shots.  The rest of the GPU suite checks the default form
-against the oracle; the one-step form is checked against it here too."""
+against the oracle; the two-step form is checked against it here too."""
 import numpy as np
 import pytest
 
@@ -29,13 +29,14 @@ def _same(got, want, what, allow_zero=False):
 
 
 def _both(engine, fn):
-    """fn() with one step per launch, then with two; the engine is left in the default form."""
+    """fn() with one step per launch, then with two; the engine is left in its
+    default form (one step per launch)."""
+    one = fn()
     try:
-        engine.set_steps_per_launch(1)
-        one = fn()
-    finally:
         engine.set_steps_per_launch(2)
-    two = fn()
+        two = fn()
+    finally:
+        engine.set_steps_per_launch(1)
     return one, two
 
 

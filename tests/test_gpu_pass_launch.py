@@ -34,7 +34,7 @@ def _model(engine, c):
 def _both(engine, fn):
     """fn() with one launch per pass, then with one launch per time step, and
     the engine's launch counts of each; the engine is left in its default
-    form (two steps per launch)."""
+    form (one step per launch)."""
     out = []
     try:
         for on in (True, False):
@@ -45,7 +45,7 @@ def _both(engine, fn):
             out.append((r, engine.stats()["launches"]))
     finally:
         engine.set_pass_launch(_DEFAULT)
-        engine.set_steps_per_launch(2)
+        engine.set_steps_per_launch(1)
     return out
 
 
