@@ -252,6 +252,7 @@ FORMS = [
     dict(name="batch_bf16_ks4", precision=2, ks=4, slots=8),
     dict(name="batch_fp32", precision=0, ks=1, slots=2),
     dict(name="fp32_checkpoint_k100", precision=0, ks=1, slots=0, ckpt=100),
+    dict(name="fp32_reconstruct", precision=0, ks=1, slots=0, recon=True),
 ]
 
 
@@ -339,6 +340,7 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         ckpt = f.get("ckpt", 0)
         n = 2 * slots if slots else 4
         engine.set_checkpointing(ckpt)
+        engine.set_reconstruction(f.get("recon", False))
         engine.set_steps_per_launch(f.get("spl", 1))
         sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
 
@@ -363,6 +365,7 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         engine.set_checkpointing(0)
+        engine.set_reconstruction(False)
         engine.set_steps_per_launch(1)
         v = n / (e0.elapsed_time(e1) / 1e3)
         out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
@@ -372,6 +375,8 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
             out[name]["checkpoint_interval"] = ckpt
         if f.get("spl", 1) != 1:
             out[name]["steps_per_launch"] = f["spl"]
+        if f.get("recon"):
+            out[name]["source_wavefield"] = "reconstructed from a saved 3-cell band"
     return out
 
 
@@ -513,8 +518,9 @@ def time_config4(engine, torch, dev, stream, peak, nshots=24):
 def time_config5(engine, torch, dev, stream, peak):
     """Config 5: one shot of the 3000 x 16000 model at 5 m (dt 0.4 ms, nt
     12000, 960 channels, 12 km streamer): FP32 snapshots (377 GB) do not fit,
-    so the forms are binary16 snapshots every 4 steps and FP32 with
-    checkpoints every 100 steps."""
+    so the forms are binary16 snapshots every 4 steps, FP32 with checkpoints
+    every 100 steps, and FP32 with the source wavefield reconstructed from a
+    saved band."""
     from psdm_b200 import rtm, synth
     ny, nx, dd, dt, nt, dpml, f0 = 3000, 16000, 5.0, 4e-4, 12000, 50, 25.0
     sv = synth.config5_survey(1)
@@ -533,9 +539,11 @@ def time_config5(engine, torch, dev, stream, peak):
     d_obs = torch.from_numpy(obs).to(dev)
     d_img = torch.zeros((nx_w, ny), dtype=torch.float32, device=dev)
     out = {"workload": f"rtm_config5_3000x16000_dx5_nt12000_cpml50_960ch_window{nx_w}"}
-    for name, precision, ks, ckpt in (("fp16_ks4", 1, 4, 0), ("fp32_checkpoint_k100", 0, 1, 100)):
+    for name, precision, ks, ckpt in (("fp16_ks4", 1, 4, 0), ("fp32_checkpoint_k100", 0, 1, 100),
+                                      ("fp32_reconstruct", 0, 1, -1)):
         prm = rtm.Params(dPML=dpml, fs=1, strategy=1, precision=precision)
-        engine.set_checkpointing(ckpt)
+        engine.set_checkpointing(max(ckpt, 0))
+        engine.set_reconstruction(ckpt < 0)
         run = lambda: engine.rtm_shot_device(prm, nxS, nyS, nxR, nyR, d_src.data_ptr(), d_obs.data_ptr(), dd, dt, ny,
                                              nx, nx_w, d_vp.data_ptr(), ADDED_SPACE, ks, nt, nt, nt, 0, 1, 0,
                                              d_img.data_ptr())
@@ -543,12 +551,16 @@ def time_config5(engine, torch, dev, stream, peak):
             rate = _shot_rate(torch, dev, stream, run, 1)
         finally:
             engine.set_checkpointing(0)
+            engine.set_reconstruction(False)
         if precision:
             fb, bb, g = algorithmic_bytes_mixed(ny, nx_w, dpml, 1, ks)
             nbytes = (fb + bb) * (nt - 1)
-        else:  # the forward pass runs twice
+        elif ckpt > 0:  # the forward pass runs twice
             fb, bb, g = algorithmic_bytes(ny, nx_w, dpml, 1)
             nbytes = (2 * fb + bb) * (nt - 1)
+        else:  # no snapshot traffic; the reverse step reads p, p1, c2 and writes p and a snapshot
+            fb, bb, g = algorithmic_bytes(ny, nx_w, dpml, 1)
+            nbytes = (fb + bb - 8 * g["n_int"] + 20 * g["n_int"]) * (nt - 1)
         cells = 2 * (nt - 1) * g["n_pad"]
         out[name] = _config_line("config5", rate, 1, cells, nbytes, peak)
         engine.trim()

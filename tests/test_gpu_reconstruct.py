@@ -2,9 +2,9 @@
 (psdm_engine_set_reconstruction): the image against the plain FP32 shot's
 (every snapshot kept) and against the oracle.  The reverse recursion repeats
 the forward step's rounding in the opposite direction, so the bar is a
-tolerance: image rel-L2 <= 1e-4 against the exact image, with the measured
-value printed; both statement orders, with and without a free surface, a
-taper, and config 1 at full size."""
+tolerance: image rel-L2 <= 2e-5 against the exact image (measured 1e-6 to
+3e-6), with the measured value printed; both statement orders, with and
+without a free surface, a taper, and config 1 at full size."""
 import numpy as np
 import pytest
 
@@ -42,7 +42,7 @@ def test_reconstruction_vs_plain(engine, ci):
     peak = np.abs(got - want).max() / np.abs(want).max()
     print(f"\nreconstruction case {ci}: image rel-L2 {rel:.2e}, peak {peak:.2e}")
     assert np.abs(want).max() > 0
-    assert rel <= 1e-4, rel
+    assert rel <= 2e-5, rel
 
 
 def test_reconstruction_config1(engine, oracle):
@@ -69,4 +69,4 @@ def test_reconstruction_config1(engine, oracle):
                            nt_snap=NT, nt_prop2=NT, nt_taper=NT)
     rel = np.linalg.norm(got - want) / np.linalg.norm(want)
     print(f"\nreconstruction config 1 (nt 3000): image rel-L2 {rel:.2e} against the oracle")
-    assert rel <= 1e-4, rel
+    assert rel <= 2e-5, rel
