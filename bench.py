@@ -558,9 +558,9 @@ def time_config5(engine, torch, dev, stream, peak):
         elif ckpt > 0:  # the forward pass runs twice
             fb, bb, g = algorithmic_bytes(ny, nx_w, dpml, 1)
             nbytes = (2 * fb + bb) * (nt - 1)
-        else:  # no snapshot traffic; the reverse step reads p, p1, c2 and writes p and a snapshot
+        else:  # forward without snapshot writes; the reverse step reads p, p1, c2 and writes p and a snapshot
             fb, bb, g = algorithmic_bytes(ny, nx_w, dpml, 1)
-            nbytes = (fb + bb - 8 * g["n_int"] + 20 * g["n_int"]) * (nt - 1)
+            nbytes = (fb - 4 * g["n_int"] + bb + 20 * g["n_int"]) * (nt - 1)
         cells = 2 * (nt - 1) * g["n_pad"]
         out[name] = _config_line("config5", rate, 1, cells, nbytes, peak)
         engine.trim()
