@@ -250,6 +250,7 @@ FORMS = [
     dict(name="fp16_ks4", precision=1, ks=4, slots=0),
     dict(name="batch_fp16_ks4", precision=1, ks=4, slots=8),
     dict(name="batch_bf16_ks4", precision=2, ks=4, slots=8),
+    dict(name="batch_fp16_ks4_two_steps", precision=1, ks=4, slots=8, spl=2),
     dict(name="batch_fp32", precision=0, ks=1, slots=2),
     dict(name="fp32_checkpoint_k100", precision=0, ks=1, slots=0, ckpt=100),
     dict(name="fp32_reconstruct", precision=0, ks=1, slots=0, recon=True),
@@ -402,10 +403,13 @@ def _config_line(name, rate, shots, cells_steps, bytes_per_shot, peak, **extra):
     return d
 
 
-def time_config1(engine, torch, dev, stream, peak, with_cpu):
+def time_config1(engine, torch, dev, stream, peak, with_cpu, mixed=False):
     """Config 1 in full: its 4 shots (200 x 600 at 10 m, CPML 40, nt 3000,
     120 channels), plain FP32 one shot at a time and all 4 in flight; and the
-    CPU restatement running the 4 shots in parallel processes."""
+    CPU restatement running the 4 shots in parallel processes.  With mixed,
+    also the mixed-precision form on the same shots (binary16 and bfloat16
+    snapshots every 4 steps, Kahan image), one at a time and all 4 in flight;
+    returned as a second entry."""
     from oracle import oracle as O
     from psdm_b200 import rtm, synth
     ny, nx, dd, dt, nt, dpml, f0 = 200, 600, 10.0, 1e-3, 3000, 40, 15.0
@@ -427,17 +431,17 @@ def time_config1(engine, torch, dev, stream, peak, with_cpu):
                           d_vp=torch.from_numpy(vmw).to(dev), d_obs=torch.from_numpy(obs).to(dev),
                           d_img=torch.zeros((nx_w, ny), dtype=torch.float32, device=dev)))
 
-    def one_at_a_time():
+    def one_at_a_time(prm=prm, ks=1):
         for it in items:
             engine.rtm_shot_device(prm, it["nxSou"], it["nySou"], it["nxRec"], it["nyRec"], d_src.data_ptr(),
                                    it["d_obs"].data_ptr(), dd, dt, ny, nx, it["nx_w"], it["d_vp"].data_ptr(),
-                                   ADDED_SPACE, 1, nt, nt, nt, 0, 1, 0, it["d_img"].data_ptr())
+                                   ADDED_SPACE, ks, nt, nt, nt, 0, 1, 0, it["d_img"].data_ptr())
 
-    def batched():
+    def batched(prm=prm, ks=1):
         descs = [dict(nxSou=it["nxSou"], nySou=it["nySou"], nxRec=it["nxRec"], nyRec=it["nyRec"], nx_w=it["nx_w"],
                       nt_prop2=nt, nt_taper=nt, d_Vp_w=it["d_vp"].data_ptr(), d_Data_target=it["d_obs"].data_ptr(),
                       d_PSDM_w=it["d_img"].data_ptr()) for it in items]
-        engine.rtm_batch_device(prm, descs, d_src.data_ptr(), dd, dt, ny, nx, ADDED_SPACE, store_snap=1,
+        engine.rtm_batch_device(prm, descs, d_src.data_ptr(), dd, dt, ny, nx, ADDED_SPACE, store_snap=ks,
                                 max_slots=len(items))
 
     fb, bb, g = algorithmic_bytes(ny, items[0]["nx_w"], dpml, 0)
@@ -456,7 +460,18 @@ def time_config1(engine, torch, dev, stream, peak, with_cpu):
         wall = time.perf_counter() - t0
         out["cpu"] = {"shots_per_s": len(items) / wall, "processes": len(items), "host_cores": host_cores(),
                       "kind": "port", "sample": "the 4 shots in full, one process each (includes process start)"}
-    return out
+    if not mixed:
+        return out, None
+    mx = {"workload": "rtm_config3_config1_shots_fp16_bf16_snapshots_ks4_kahan_image"}
+    mb, mbb, _ = algorithmic_bytes_mixed(ny, items[0]["nx_w"], dpml, 0, 4)
+    for kind, name in ((1, "fp16"), (2, "bf16")):
+        pm = rtm.Params(dPML=dpml, fs=0, strategy=1, precision=kind)
+        for form, fn in (("one_at_a_time", one_at_a_time), ("batched_4", batched)):
+            r = _shot_rate(torch, dev, stream, lambda: fn(pm, 4), len(items))
+            base = out["gpu_" + form]["shots_per_s"]
+            mx[f"{name}_ks4_{form}"] = _config_line("config3", r, len(items), cells, (mb + mbb) * (nt - 1), peak,
+                                                    vs_plain_fp32=r / base)
+    return out, mx
 
 
 def _cpu_config1_worker(args):
@@ -701,13 +716,18 @@ def run_gpu(args):
     if world == 1 and names:
         forms = time_forms(engine, torch, dev, stream, d_src, items_u, names, value)
     configs = None
-    cnames = ["config1", "config4", "config5"] if args.configs == "all" else \
+    cnames = ["config1", "config3", "config4", "config5"] if args.configs == "all" else \
         [n for n in args.configs.split(",") if n and n != "none"]
     if world == 1 and cnames:
         peak_c, _ = _peaks()
         configs = {}
-        if "config1" in cnames:
-            configs["config1"] = time_config1(engine, torch, dev, stream, peak_c, not args.no_cpu)
+        if "config1" in cnames or "config3" in cnames:
+            c1, c3 = time_config1(engine, torch, dev, stream, peak_c, not args.no_cpu and "config1" in cnames,
+                                  mixed="config3" in cnames)
+            if "config1" in cnames:
+                configs["config1"] = c1
+            if c3 is not None:
+                configs["config3"] = c3
         if "config4" in cnames:
             configs["config4"] = time_config4(engine, torch, dev, stream, peak_c)
         if "config5" in cnames:
@@ -766,8 +786,8 @@ def main():
                     help="other engine forms to time after the drop-in: all, none or a comma list of " +
                          ", ".join(f["name"] for f in FORMS))
     ap.add_argument("--configs", default="all",
-                    help="other benchmark configurations to time: all, none or a comma list of config1, config4, "
-                         "config5")
+                    help="other benchmark configurations to time: all, none or a comma list of config1, config3, "
+                         "config4, config5")
     ap.add_argument("--nt", type=int, default=None,
                     help="override the record length (small cases for ncu captures only; not a bench value)")
     args = ap.parse_args()

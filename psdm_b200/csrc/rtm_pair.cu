@@ -357,6 +357,36 @@ struct GenTile {
     int z0, z1, x0, x1;
 };
 
+// Snapshot store (forward) or imaging update (backward) of interior cell fi
+// of the migration window at sub-step SUB, from its level n+1+SUB value and
+// its level n+SUB-1 value pmo.
+template <int MODE, int SUB>
+__device__ __forceinline__ void pair_field(const PairArgs& P, int fi, float out, float pmo) {
+    const StepArgs& a = P.a;
+    const SubStep& s = P.sub[SUB];
+    if (MODE == 0) {
+        if (s.field != nullptr) {
+            const float D = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
+            s.field[fi] = D;
+            if (s.field_amax != nullptr) atomicMax(&s_pair_amax[SUB], __float_as_uint(fabsf(D)));
+        }
+    } else if (MODE == 1) {
+        if (s.field != nullptr) {
+            float F = __ldg(s.field + fi);
+            if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
+            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
+            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+            a.image[fi] = __fadd_rn(a.image[fi], inc);
+        }
+    } else if (s.field16 != nullptr) {
+        float F = load16x1(s.field16, fi, a.kind16, __ldg(s.field_iscale));
+        if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
+        float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
+        if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
+        kahan(a.image[fi], a.comp[fi], inc);
+    }
+}
+
 // One cell of a generic tile at sub-step SUB: the one-step kernels' generic
 // cell update (rtm_step.cu, cell_generic) with its sources moved:
 //   SUB 0: stencil level n from S0, level n-1 / phi / chi at level n and the
@@ -522,30 +552,7 @@ __device__ __forceinline__ void pair_cell(const PairArgs& P, const GenTile& G, i
         else if (kx == 0 && kz >= 1 && kz <= 3)
             s.band[6 * a.ny + (x - dn) * 6 + (z >= dn + a.ny ? z - (dn + a.ny) : 3 + z - (dn - 3))] = out;
     }
-    if (inT && kx == 0 && kz == 0) {
-        const int fi = (x - dn) * a.ldf + (z - dn);
-        if (MODE == 0) {
-            if (s.field != nullptr) {
-                const float D = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
-                s.field[fi] = D;
-                if (s.field_amax != nullptr) atomicMax(&s_pair_amax[SUB], __float_as_uint(fabsf(D)));
-            }
-        } else if (MODE == 1) {
-            if (s.field != nullptr) {
-                float F = __ldg(s.field + fi);
-                if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
-                float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
-                if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
-                a.image[fi] = __fadd_rn(a.image[fi], inc);
-            }
-        } else if (s.field16 != nullptr) {
-            float F = load16x1(s.field16, fi, a.kind16, __ldg(s.field_iscale));
-            if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
-            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
-            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
-            kahan(a.image[fi], a.comp[fi], inc);
-        }
-    }
+    if (inT && kx == 0 && kz == 0) pair_field<MODE, SUB>(P, (x - dn) * a.ldf + (z - dn), out, pmo);
 }
 
 // Tile bounds of generic rect r, tile t: an even split of the rect into
@@ -606,6 +613,195 @@ __device__ __forceinline__ void pair_generic_tile(const PairArgs& P, float* sm, 
         gather_receivers(P, b, G.S0, G.z0 - 6, G.x0 - 6, GH0, G.S1, G.z0 - 3, G.x0 - 3, GH1);
 }
 
+// ---- x-strip tiles (rect type 2): the C-PML x-strips beside a clean run
+//
+// Rows of a clean run (interior rows away from the free surface and the
+// injection rows, float4-aligned), columns of one x-strip.  Every cell of
+// the tile and its 3-cell ring has kz = 0; the ring reaches 3 interior
+// columns on the strip's inner side.  A thread owns a float4 of rows of one
+// column at a time (16 float4 rows of the first step per half-warp, two
+// columns per warp), so the C-PML factors and the clamped stencil centres
+// are uniform per half-warp and every operand moves as a float4.
+constexpr int XZ = 56, XX = 28;              // tile rows (a multiple of 4) and columns at most
+constexpr int XQ0 = (XZ + 16) / 4;           // float4 rows of level n (rows from z0-8)
+constexpr int XQ1 = (XZ + 8) / 4;            // float4 rows of level n+1 (rows from z0-4)
+constexpr int XW0 = XX + 12, XW1 = XX + 6;   // columns of level n (from x0-6) and n+1 (from x0-3)
+constexpr int kXStripFloats = 4 * (XQ0 * XW0 + 3 * XQ1 * XW1);
+static_assert(kXStripFloats <= kPairFloats, "x-strip tiles fit the launch's shared memory");
+
+__host__ __device__ __forceinline__ void xstrip_bounds(const PairArgs& P, int r, int t, int* z0, int* z1, int* x0,
+                                                       int* x1) {
+    const int nz = P.r_tz[r], nxr = P.r_tx[r], nq = P.r_h[r] / 4;
+    const int tz = t % nz, tx = t / nz;
+    *z0 = P.r_zd0[r] + 4 * ((tz * nq) / nz);
+    *z1 = P.r_zd0[r] + 4 * (((tz + 1) * nq) / nz);
+    *x0 = P.r_x0[r] + (tx * P.r_w[r]) / nxr;
+    *x1 = P.r_x0[r] + ((tx + 1) * P.r_w[r]) / nxr;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st4(float* p, const float4& v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 f4(const float (&v)[4]) { return make_float4(v[0], v[1], v[2], v[3]); }
+
+// One float4 of an x-strip tile at step SUB: rows zd..zd+3 (device), column x.
+//   SUB 0: level n from S0 (float4 rows from z0-8, columns from x0-6);
+//     phi, chi, p1 at level n from HBM; results into S1 / F1 / X1 (float4
+//     rows from z0-4, columns from x0-3) and, on the tile, to the level n+1
+//     outputs.
+//   SUB 1: level n+1 from S1 / F1 / X1, p1 = level n from S0; results to the
+//     level n+2 outputs and over level n in S0.
+template <int MODE, int SUB>
+__device__ __forceinline__ void xstrip_quad(const PairArgs& P, float4* S0, float4* S1, float4* F1, float4* X1,
+                                            int z0, int x0, int x1, int zd, int x, bool inT) {
+    const StepArgs& a = P.a;
+    const SubStep& s = P.sub[SUB];
+    const int dn = a.dn;
+    const int kx = (x < dn) ? (dn - x) : (x >= dn + a.nx ? x - (dn + a.nx) + 1 : 0);
+    const int cx = clampi(x, 3, a.nxt - 4);
+    const float4* SS = SUB == 0 ? S0 : S1;
+    const int QS = SUB == 0 ? XQ0 : XQ1;
+    const int ox = SUB == 0 ? x0 - 6 : x0 - 3;
+    const int rs = SUB == 0 ? (zd - (z0 - 8)) >> 2 : (zd - (z0 - 4)) >> 2;  // float4 row in the source
+    const int r1 = (zd - (z0 - 4)) >> 2;                                      // float4 row in S1 / F1 / X1
+    float4 W[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) W[k] = SS[(cx - 3 + k - ox) * QS + rs];
+    const float4 zc = SS[(x - ox) * QS + rs];
+    const float4 zm = SS[(x - ox) * QS + rs - 1];
+    const float4 zp = SS[(x - ox) * QS + rs + 1];
+    const int g = x * a.ldz + zd;
+    const float4 pmv = SUB == 0 ? ld4(a.pm + g) : S0[(x - (x0 - 6)) * XQ0 + ((zd - (z0 - 8)) >> 2)];
+    const float4 c2v = ld4(a.c2 + g);
+    const float zv[10] = {zm.y, zm.z, zm.w, zc.x, zc.y, zc.z, zc.w, zp.x, zp.y, zp.z};
+    float o[4], phn[4], chn[4];
+    if (kx > 0) {
+        const int sb = (x < dn) ? 0 : dn + a.nx;
+        const int ci = clampi(x - sb, 3, dn - 4) + sb;
+        float4 F[7];
+        float4 phc, chc;
+        if (SUB == 0) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if (k != 3) F[k] = ld4(a.phix_in + (size_t)(ci - 3 + k) * a.ldz + zd);
+            phc = ld4(a.phix_in + g);
+            chc = ld4(P.chix_in + g);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if (k != 3) F[k] = F1[(ci - 3 + k - (x0 - 3)) * XQ1 + r1];
+            phc = F1[(x - (x0 - 3)) * XQ1 + r1];
+            chc = X1[(x - (x0 - 3)) * XQ1 + r1];
+        }
+        F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float A = __ldg(a.fA + kx - 1), B = __ldg(a.fB + kx - 1);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+#define PXR(k) comp(W[3 + (k)], e)
+#define FXR(k) comp(F[3 + (k)], e)
+#define ZR(k) zv[3 + e + (k)]
+            const float d2x = D2(PXR, a.cf2);
+            const float d1x = D1(PXR, a.cf1);
+            const float d2y = D2(ZR, a.cf2);
+            const float dph = D1(FXR, a.cf1);
+#undef PXR
+#undef FXR
+#undef ZR
+            phn[e] = __fadd_rn(__fmul_rn(A, comp(phc, e)), __fmul_rn(B, d1x));
+            chn[e] = __fadd_rn(__fmul_rn(A, comp(chc, e)), __fmul_rn(B, __fadd_rn(d2x, dph)));
+            const float prop = __fadd_rn(dph, chn[e]);
+            const float base = __fadd_rn(-comp(pmv, e), __fmul_rn(2.f, comp(zc, e)));
+            o[e] = __fadd_rn(base, __fmul_rn(comp(c2v, e), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+        }
+    } else {  // an interior column of the ring: no C-PML term, no injection here
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+#define PXR(k) comp(W[3 + (k)], e)
+#define ZR(k) zv[3 + e + (k)]
+            const float d2x = D2(PXR, a.cf2);
+            const float d2y = D2(ZR, a.cf2);
+#undef PXR
+#undef ZR
+            const float base = __fadd_rn(-comp(pmv, e), __fmul_rn(2.f, comp(zc, e)));
+            o[e] = __fadd_rn(base, __fmul_rn(comp(c2v, e), __fadd_rn(__fadd_rn(d2x, d2y), 0.f)));
+            phn[e] = chn[e] = 0.f;
+        }
+    }
+    const float4 out = f4(o);
+    if (SUB == 0) {
+        S1[(x - (x0 - 3)) * XQ1 + r1] = out;
+        if (kx > 0) {
+            F1[(x - (x0 - 3)) * XQ1 + r1] = f4(phn);
+            X1[(x - (x0 - 3)) * XQ1 + r1] = f4(chn);
+        }
+        if (inT) {
+            st4(P.p_out[0] + g, out);
+            if (P.nsub == 1) {
+                st4(a.phix_out + g, f4(phn));
+                st4(a.chix + g, f4(chn));
+            }
+        }
+    } else {
+        st4(P.p_out[1] + g, out);
+        st4(a.phix_out + g, f4(phn));
+        st4(a.chix + g, f4(chn));
+        S0[(x - (x0 - 6)) * XQ0 + ((zd - (z0 - 8)) >> 2)] = out;
+    }
+    if (inT && kx == 0) {
+        const int fi = (x - dn) * a.ldf + (zd - a.zoff - dn);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) pair_field<MODE, SUB>(P, fi + e, o[e], comp(pmv, e));
+    }
+    if (MODE == 0 && inT && s.band != nullptr && kx >= 1 && kx <= 3) {
+        const int z = zd - a.zoff;
+        float* bp = s.band + (x < dn ? x - (dn - 3) : 3 + x - (dn + a.nx)) * a.ny + (z - dn);
+        bp[0] = o[0];
+        bp[1] = o[1];
+        bp[2] = o[2];
+        bp[3] = o[3];
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void pair_xstrip_tile(const PairArgs& P, float* sm, int r, int t, int b) {
+    const StepArgs& a = P.a;
+    int z0, z1, x0, x1;
+    xstrip_bounds(P, r, t, &z0, &z1, &x0, &x1);
+    float4* S0 = reinterpret_cast<float4*>(sm);
+    float4* S1 = S0 + XQ0 * XW0;
+    float4* F1 = S1 + XQ1 * XW1;
+    float4* X1 = F1 + XQ1 * XW1;
+    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int H = z1 - z0, W = x1 - x0;
+    // level n on rows [z0-8, z1+8) x columns [x0-6, x1+6), zero outside the grid
+    const int nq0 = H / 4 + 4, W0 = W + 12;
+    for (int i = tid; i < nq0 * W0; i += NT) {
+        const int c = i / nq0, q = i - c * nq0;
+        const int x = x0 - 6 + c;
+        S0[c * XQ0 + q] = (x >= 0 && x < a.nxt) ? ld4(a.p + (size_t)x * a.ldz + (z0 - 8) + 4 * q)
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    // first step: float4 rows [z0-4, z1+4) (16 per half-warp) x the columns
+    // of [x0-3, x1+3) inside the grid, two columns per warp at a time
+    const int hq = lane & 15, hc = (w << 1) | (lane >> 4);  // float4 row, column slot 0..7
+    const int cl = max(x0 - 3, 0), cr = min(x1 + 3, a.nxt);
+    if (hq < H / 4 + 2)
+        for (int x = cl + hc; x < cr; x += 2 * NWARP) {
+            const int zd = z0 - 4 + 4 * hq;
+            const bool inT = hq >= 1 && hq <= H / 4 && x >= x0 && x < x1;
+            xstrip_quad<MODE, 0>(P, S0, S1, F1, X1, z0, x0, x1, zd, x, inT);
+        }
+    if (P.nsub == 2) {
+        __syncthreads();
+        if (hq < H / 4)
+            for (int x = x0 + hc; x < x1; x += 2 * NWARP)
+                xstrip_quad<MODE, 1>(P, S0, S1, F1, X1, z0, x0, x1, z0 + 4 * hq, x, true);
+    }
+    if (MODE == 0 && P.rec_first != nullptr)
+        gather_receivers(P, b, reinterpret_cast<float*>(S0), z0 - 8, x0 - 6, 4 * XQ0, reinterpret_cast<float*>(S1),
+                         z0 - 4, x0 - 3, 4 * XQ1);
+}
+
 // Tile b of a launch; false if its bulk copies did not complete.
 template <int MODE>
 __device__ __forceinline__ bool pair_tile(const PairArgs& P, float* sm, uint64_t* bar, uint32_t& phase, int b) {
@@ -613,7 +809,10 @@ __device__ __forceinline__ bool pair_tile(const PairArgs& P, float* sm, uint64_t
     while (r + 1 < P.nrect && b >= P.r_first[r + 1]) ++r;
     const int t = b - P.r_first[r];
     if (P.r_type[r] == 0) return pair_clean_tile<MODE>(P, sm, bar, phase, r, t, b);
-    pair_generic_tile<MODE>(P, sm, r, t, b);
+    if (P.r_type[r] == 2)
+        pair_xstrip_tile<MODE>(P, sm, r, t, b);
+    else
+        pair_generic_tile<MODE>(P, sm, r, t, b);
     return true;
 }
 
@@ -931,8 +1130,8 @@ bool plan_pair(PairArgs* P, const int* row_slot_host) {
         P->r_x0[n] = x0;
         P->r_h[n] = h;
         P->r_w[n] = w;
-        P->r_tz[n] = type == 0 ? (h + TZC - 1) / TZC : (h + GZ - 1) / GZ;
-        P->r_tx[n] = type == 0 ? (w + TXC - 1) / TXC : (w + GX - 1) / GX;
+        P->r_tz[n] = type == 0 ? (h + TZC - 1) / TZC : type == 2 ? (h / 4 + XZ / 4 - 1) / (XZ / 4) : (h + GZ - 1) / GZ;
+        P->r_tx[n] = type == 0 ? (w + TXC - 1) / TXC : type == 2 ? (w + XX - 1) / XX : (w + GX - 1) / GX;
         P->r_first[n + 1] = P->r_first[n] + P->r_tz[n] * P->r_tx[n];
         ++n;
     };
@@ -942,14 +1141,14 @@ bool plan_pair(PairArgs* P, const int* row_slot_host) {
         if (za < top || zb > bot) continue;
         bool clean = false;
         for (auto& rn : runs) clean = clean || (rn.first == za && rn.second == zb);
-        add(1, za, 0, zb - za, dn);
-        if (clean) {
-            add(1, za, dn, zb - za, cx0 - dn);
-            add(1, za, cx1, zb - za, dn + nx - cx1);
+        if (clean) {  // the x-strips and the 3 interior columns beside them, float4 tiles
+            add(2, za, 0, zb - za, cx0);
+            add(2, za, cx1, zb - za, nxt - cx1);
         } else {
+            add(1, za, 0, zb - za, dn);
             add(1, za, dn, zb - za, nx);
+            add(1, za, dn + nx, zb - za, nxt - (dn + nx));
         }
-        add(1, za, dn + nx, zb - za, nxt - (dn + nx));
     }
     P->nrect = n;
     return !overflow;
@@ -965,6 +1164,8 @@ void pair_tile_rect(const PairArgs& P, int b, int* z0, int* z1, int* x0, int* x1
         *x0 = P.r_x0[r] + tx * P.txc;
         *z1 = std::min(*z0 + TZC, P.r_zd0[r] + P.r_h[r]);
         *x1 = std::min(*x0 + P.txc, P.r_x0[r] + P.r_w[r]);
+    } else if (P.r_type[r] == 2) {
+        xstrip_bounds(P, r, t, z0, z1, x0, x1);
     } else {
         generic_bounds(P, r, t, z0, z1, x0, x1);
     }

@@ -5,6 +5,8 @@
 // Usage: pair_plan_check ny nx dPML fs nrec [injection rows (0-based interior rows)...]
 // Prints: ntiles nclean cover_errors shape_errors clean_errors reach_errors rec_errors
 //
+// x-strip tiles (type 2): rows of a clean run, float4-aligned, at most 56 x 28.
+//
 // reach: every read of a tile's second step (the clamped x / z stencils of
 // level n+1 and the strip-local phi stencils, rtm_pair.cu) lies in the tile
 // plus a 3-cell ring, where the first step computes level n+1, and every
@@ -65,7 +67,7 @@ int main(int argc, char** argv) {
         pair_tile_rect(P, b, &z0, &z1, &x0, &x1);
         int r = 0;
         while (r + 1 < P.nrect && b >= P.r_first[r + 1]) ++r;
-        const bool clean = P.r_type[r] == 0;
+        const bool clean = P.r_type[r] == 0, xs = P.r_type[r] == 2;
         nclean += clean;
         if (z0 >= z1 || x0 >= x1 || z0 < 0 || x0 < 0 || z1 > a.ldz || x1 > a.nxt) {
             ++shape_err;
@@ -82,11 +84,20 @@ int main(int argc, char** argv) {
                     if (z < dn || z >= dn + ny || x < dn || x >= dn + nx || (fs && z == dn) || inj_row[z])
                         ++clean_err;
                 }
+        } else if (xs) {
+            if (z0 % 4 || (z1 - z0) % 4 || z1 - z0 > 56 || x1 - x0 > 28) ++shape_err;
+            // float4 loads of level n on rows [z0-8, z1+8) inside the arrays
+            if (z0 - 8 < 0 || z1 + 8 > a.ldz) ++shape_err;
+            // rows of the tile and its ring: interior, no free surface, no injection
+            for (int zd = z0 - 3; zd < z1 + 3; ++zd) {
+                const int z = zd - a.zoff;
+                if (z < dn || z >= dn + ny || (fs && z == dn) || inj_row[z]) ++clean_err;
+            }
         } else if (z1 - z0 > 26 || x1 - x0 > 32) {
             ++shape_err;
         }
-        // level-n cells a tile has: generic tile + 6; clean: the staged block
-        const int lz0 = clean ? z0 - 8 : z0 - 6, lz1 = clean ? z1 + 8 : z1 + 6;
+        // level-n cells a tile has: generic tile + 6; clean and x-strip: rows + 8
+        const int lz0 = (clean || xs) ? z0 - 8 : z0 - 6, lz1 = (clean || xs) ? z1 + 8 : z1 + 6;
         const int lx0 = x0 - 6, lx1 = x1 + 6;
         auto in_ring3 = [&](int zd, int x) { return zd >= z0 - 3 && zd < z1 + 3 && x >= x0 - 3 && x < x1 + 3; };
         auto in_load = [&](int zd, int x) { return zd >= lz0 && zd < lz1 && x >= lx0 && x < lx1; };
