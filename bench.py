@@ -535,7 +535,8 @@ def time_config5(engine, torch, dev, stream, peak):
     12000, 960 channels, 12 km streamer): FP32 snapshots (377 GB) do not fit,
     so the forms are binary16 snapshots every 4 steps, FP32 with checkpoints
     every 100 steps, and FP32 with the source wavefield reconstructed from a
-    saved band."""
+    saved band, one shot at a time; and batched binary16 with every snapshot
+    and with checkpoints."""
     from psdm_b200 import rtm, synth
     ny, nx, dd, dt, nt, dpml, f0 = 3000, 16000, 5.0, 4e-4, 12000, 50, 25.0
     sv = synth.config5_survey(1)
@@ -580,6 +581,39 @@ def time_config5(engine, torch, dev, stream, peak):
         out[name] = _config_line("config5", rate, 1, cells, nbytes, peak)
         engine.trim()
     out["fp32_all_snapshots"] = {"fits": False, "snapshot_gb": round(4.0 * ny * nx_w * (nt - 1) / 1e9, 1)}
+    # Batched binary16 every 4 steps: every snapshot kept (as many shots in
+    # flight as fit), and with checkpoints at the planner's interval (more
+    # shots in flight, the forward pass twice).  The shots repeat shot 0's
+    # geometry and data.
+    prm = rtm.Params(dPML=dpml, fs=1, strategy=1, precision=1)
+    fb, bb, g = algorithmic_bytes_mixed(ny, nx_w, dpml, 1, 4)
+    fb32, _, _ = algorithmic_bytes(ny, nx_w, dpml, 1)
+    cells = 2 * (nt - 1) * g["n_pad"]
+    engine.trim()
+    torch.cuda.synchronize(dev)
+    free, _ = torch.cuda.mem_get_info(dev)
+    for name, force_ckpt in (("batch_fp16_ks4", False), ("batch_fp16_ks4_checkpoint", True)):
+        budget = free if not force_ckpt else min(free, 40 * 10 ** 9)  # 40 GB per shot: below its 47 GB of snapshots
+        plan = rtm.plan_memory(prm, ny, nx_w, nt, nt, 4, len(nxR), budget)
+        if not plan["fits"]:
+            continue
+        K = plan["checkpoint_interval"]
+        slots = plan["slots"] if not force_ckpt else min(8, int((free - 2 ** 30) // plan["bytes_per_slot"]))
+        if slots < 1:
+            continue
+        descs = [dict(nxSou=nxS, nySou=nyS, nxRec=nxR, nyRec=nyR, nx_w=nx_w, nt_prop2=nt, nt_taper=nt,
+                      d_Vp_w=d_vp.data_ptr(), d_Data_target=d_obs.data_ptr(), d_PSDM_w=d_img.data_ptr())] * slots
+        engine.set_checkpointing(K)
+        run = lambda: engine.rtm_batch_device(prm, descs, d_src.data_ptr(), dd, dt, ny, nx, ADDED_SPACE, store_snap=4,
+                                              max_slots=slots)
+        try:
+            rate = _shot_rate(torch, dev, stream, run, slots)
+        finally:
+            engine.set_checkpointing(0)
+        nbytes = (fb + bb + (fb32 - 4 * g["n_int"] if K else 0)) * (nt - 1)  # checkpoints: the forward pass twice
+        out[name] = _config_line("config5", rate, slots, cells, nbytes, peak, slots=engine.batch_slots(),
+                                 checkpoint_interval=K, gb_per_shot=round(plan["bytes_per_slot"] / 1e9, 1))
+        engine.trim()
     return out
 
 

@@ -187,13 +187,16 @@ int psdm_rtm_batch_device(
     const float* d_Data_source, float dd, float dt, int32_t ny, int32_t nx, float added_space,
     int32_t store_snap, int32_t taper_option, int32_t N_taper, int32_t N_zeros, int32_t max_slots);
 /*
- * Checkpointing for FP32 shots (psdm_rtm_shot, psdm_rtm_shot_device):
- * interval K > 0 keeps the propagation state every K forward steps and
- * recomputes each K-step segment of the forward pass during the backward
- * pass, in place of holding all nt_prop2 snapshots (the role of the
- * reference's disk strategy, solver_ac_forward_disk.f90:469-517).  Same image
- * bit for bit; the forward pass runs twice.  0 (default) = off.  Not used by
- * the batched or mixed-precision forms.
+ * Checkpointing (psdm_rtm_shot, psdm_rtm_batch and their device variants,
+ * FP32 and mixed precision): interval K > 0 keeps the propagation state every
+ * K forward steps and recomputes each K-step segment of the forward pass
+ * during the backward pass, in place of holding all snapshots of the pass
+ * (the role of the reference's disk strategy,
+ * solver_ac_forward_disk.f90:469-517).  Mixed-precision segments are staged
+ * and converted to 16 bits as in the pass without checkpoints.  Same image
+ * bit for bit; the forward pass runs twice.  0 (default) = off.
+ * Reconstruction (psdm_engine_set_reconstruction) takes precedence for
+ * single FP32 shots.
  */
 int psdm_engine_set_checkpointing(psdm_engine* e, int32_t interval);
 /*
@@ -240,7 +243,7 @@ int psdm_engine_set_steps_per_launch(psdm_engine* e, int32_t steps);
 typedef struct psdm_plan {
     int32_t steps_per_launch;     /* launch form chosen (1 or 2) */
     int32_t slots;                /* shots in flight for the batched calls (1: one shot at a time) */
-    int32_t checkpoint_interval;  /* 0: all snapshots in HBM; K > 0: FP32 checkpoints every K steps */
+    int32_t checkpoint_interval;  /* 0: all snapshots in HBM; K > 0: checkpoints every K steps */
     int32_t fits;                 /* 1 if the plan fits the budget */
     int64_t bytes_per_slot;       /* device bytes of one shot in flight under the plan */
     int64_t budget_bytes;         /* the budget planned against */
@@ -251,9 +254,9 @@ typedef struct psdm_plan {
  * Memory plan of shots of a window ny x nx_w with nt_prop2 / nt_taper steps
  * (host arithmetic only, no device needed): the device bytes of one shot in
  * flight for the snapshot form that prm->precision selects; slots =
- * min(max_slots, what fits in budget_bytes less a 1 GiB reserve); for FP32
- * shots whose snapshots do not fit, the checkpoint interval K that
- * minimises their memory (one shot at a time).  Returns PSDM_ERR_NOMEM, with
+ * min(max_slots, what fits in budget_bytes less a 1 GiB reserve); for shots
+ * whose snapshots do not fit, the checkpoint interval K that minimises their
+ * memory, and the slots that fit with it.  Returns PSDM_ERR_NOMEM, with
  * the sizes in psdm_last_error(), when not even that fits.  The plan's
  * steps_per_launch is 1 and probe_us zero.
  */

@@ -97,7 +97,7 @@ struct psdm_engine {
     std::vector<int> pass_key[3];  // by pass kind (mode)
     cudaEvent_t pass_staged[3] = {nullptr, nullptr, nullptr};  // copies out of the staging buffers done
     int batch_slots = 0;  // slots used by the last batched call
-    int ckpt_interval = 0;  // > 0: FP32 shots keep checkpoints instead of all snapshots
+    int ckpt_interval = 0;  // > 0: shots keep checkpoints every K steps instead of all snapshots
     bool recon = false;     // FP32 shots reconstruct the source wavefield from a saved band
     std::map<std::pair<int, int>, std::array<int, 2>> fft_plans;  // (length, batch) -> cuFFT plans
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
@@ -1011,15 +1011,19 @@ int window_geometry(const Grid& g, int NumRec, int nxSou, int nySou, const int* 
 // sample store_snap*m.  This form has no reference counterpart; for
 // store_snap = 1 its pairing is the reference's.
 
-int mixed_bufs(psdm_engine* e, const Shot& s, int kind, int ks, int nt_prop2, const std::string& tag, MixedBufs* mb) {
+// nslots16: 16-bit snapshot slots to allocate (all nsnap of the pass when
+// negative; fewer when the slots are reused, as by checkpointed shots).
+int mixed_bufs(psdm_engine* e, const Shot& s, int kind, int ks, int nt_prop2, const std::string& tag, MixedBufs* mb,
+               int nslots16 = -1) {
     mb->kind = kind;
     mb->ks = ks;
     mb->nsnap = (nt_prop2 - 1) / ks;
     mb->fstride = s.g.field_cells();
     const size_t fs = mb->fstride, ns = (size_t)std::max(mb->nsnap, 1);
+    const size_t n16 = nslots16 < 0 ? ns : (size_t)std::max(nslots16, 1);
     for (int i = 0; i < 4; ++i) TRY(e->get(("stage" + std::to_string(i) + tag).c_str(), fs, &mb->stage[i]));
     TRY(e->get(("amax" + tag).c_str(), ns, &mb->amax));
-    TRY(e->get(("snap16" + tag).c_str(), ns * fs, &mb->snap16));
+    TRY(e->get(("snap16" + tag).c_str(), n16 * fs, &mb->snap16));
     TRY(e->get(("iscale" + tag).c_str(), ns, &mb->iscale));
     TRY(e->get(("comp" + tag).c_str(), fs, &mb->comp));
     // The staging buffers' pad rows are converted too: keep them zero.
@@ -1329,6 +1333,11 @@ int rtm_shot_reconstructed(psdm_engine* e, const psdm_params* prm, int NumRec, i
 
 // One shot of RTM with every array in device memory
 // (calculate_PSDM_RTM.f90:395-466).  Asynchronous on e->stream.
+int rtm_shot_mixed_ckpt(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
+                        const int* nyRec, const float* d_S, const float* d_tgt, float dd, float dt, int ny, int nx,
+                        int nx_w, const float* d_vp, float added_space, int store_snap, int nt_prop2, int nt_taper,
+                        int taper_option, int N_taper, int N_zeros, float* d_img);
+
 int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
                   const int* nyRec, const float* d_S, const float* d_tgt, float dd, float dt, int ny, int nx,
                   int nx_w, const float* d_vp, float added_space, int store_snap, int nt_snap, int nt_prop2,
@@ -1343,6 +1352,9 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
     if (taper_option != 0 && N_taper < 1) return fail(PSDM_ERR_ARG, "N_taper must be >= 1");
     const int nsnap = (nt_prop2 - 1) / store_snap;  // slots written by the forward pass
     if (nsnap > nt_snap) return fail(PSDM_ERR_ARG, "nt_snap=%d < %d snapshots", nt_snap, nsnap);
+    if (prm->precision != PSDM_PREC_FP32 && e->ckpt_interval > 0)
+        return rtm_shot_mixed_ckpt(e, prm, NumRec, nxSou, nySou, nxRec, nyRec, d_S, d_tgt, dd, dt, ny, nx, nx_w, d_vp,
+                                   added_space, store_snap, nt_prop2, nt_taper, taper_option, N_taper, N_zeros, d_img);
     Shot s;
     TRY(setup_shot(e, prm, ny, nx_w, dd, dt, d_vp, &s));
     WinGeom w;
@@ -1447,10 +1459,19 @@ int rtm_shot_core(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou,
 // the per-step arguments of a shot's two passes are built on the host once,
 // staged through page-locked memory and read by the kernel from HBM.
 
+// One entry of a slot's program: a step launch (batched with the other
+// slots' next launches) or a state operation between two of its launches.
+enum SlotOpKind { OP_LAUNCH, OP_SAVE, OP_RESTORE, OP_RESET, OP_RESET_F, OP_QUANT };
+struct SlotOp {
+    int kind = OP_LAUNCH;
+    int mode = 0;   // OP_LAUNCH: 0 forward, 1 backward, 2 mixed backward
+    int arg = 0;    // OP_LAUNCH: index of its arguments; OP_SAVE / OP_RESTORE: checkpoint; OP_QUANT: snapshot m
+    int tiles = 0;  // OP_LAUNCH: tiles of the launch
+    unsigned short* dst = nullptr;  // OP_QUANT: where the 16-bit snapshot goes
+};
+
 struct BatchSlot {
     int shot = -1;       // shot index, -1 = idle
-    int pass = 0;        // 0 forward, 1 backward
-    int k = 0;           // steps of the current pass done
     int nfwd = 0, nbwd = 0;
     int tiles[2] = {0, 0};
     std::string tag;
@@ -1470,6 +1491,10 @@ struct BatchSlot {
     int bwd_mode = 1;              // 1 plain backward, 2 mixed-precision backward
     MixedBufs mb;                  // mixed form: the slot's 16-bit snapshots
     int pending = 0;               // mixed form: slot taken at the last forward step
+    std::vector<SlotOp> ops;       // the shot's program
+    size_t pc = 0;                 // next entry of ops
+    Shot f;                        // checkpointed shots: the recomputed forward state
+    float* ckpts = nullptr;        // checkpointed shots: states saved every K forward steps
 };
 
 struct BatchJob {
@@ -1492,35 +1517,13 @@ int check_batch_shot(const BatchJob& j, int i) {
 }
 
 // Start shot `i` in slot `sl`: inputs, state, window, per-step arguments.
-int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
+// The program of a slot's shot with every snapshot kept (FP32 slots or the
+// mixed form's 16-bit slots): its forward launches, the conversion of the
+// last staged snapshots, a fresh wavefield, its backward launches.
+int batch_program_plain(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i, const WinGeom& w,
+                        const float* d_tgt) {
     const psdm_shot& sh = j.shots[i];
-    const int ny = j.ny, nx_w = sh.nx_w;
     const std::string& tag = sl.tag;
-    const float* d_vp = sh.Vp_w;
-    const float* d_tgt = sh.Data_target;
-    const size_t nvp = (size_t)ny * nx_w, ntgt = (size_t)sh.NumRec * sh.nt_taper;
-    // The slot's page-locked staging is reused only once its previous
-    // copies have completed.
-    CUDA_TRY(cudaEventSynchronize(sl.staged));
-    if (j.host_io) {
-        float *h_vp = nullptr, *h_tgt = nullptr, *dv = nullptr, *dtg = nullptr;
-        TRY(e->get_pinned(("hvp" + tag).c_str(), nvp * sizeof(float), (void**)&h_vp));
-        TRY(e->get_pinned(("htgt" + tag).c_str(), ntgt * sizeof(float), (void**)&h_tgt));
-        std::memcpy(h_vp, sh.Vp_w, nvp * sizeof(float));
-        std::memcpy(h_tgt, sh.Data_target, ntgt * sizeof(float));
-        TRY(e->get(("vp" + tag).c_str(), nvp, &dv));
-        TRY(e->get(("tgt" + tag).c_str(), ntgt, &dtg));
-        CUDA_TRY(cudaMemcpyAsync(dv, h_vp, nvp * sizeof(float), cudaMemcpyHostToDevice, e->stream));
-        CUDA_TRY(cudaMemcpyAsync(dtg, h_tgt, ntgt * sizeof(float), cudaMemcpyHostToDevice, e->stream));
-        d_vp = dv;
-        d_tgt = dtg;
-    }
-    TRY(setup_shot(e, j.prm, ny, nx_w, j.dd, j.dt, d_vp, &sl.s, tag));
-    WinGeom w;
-    TRY(window_geometry(sl.s.g, sh.NumRec, sh.nxSou, sh.nySou, sh.nxRec, sh.nyRec, j.dd, j.nx, j.added_space, &w));
-    if (w.nx_w_calc != nx_w)
-        return fail(PSDM_ERR_ARG, "shot %d: nx_w=%d does not match the window of its geometry (%d)", i, nx_w,
-                    w.nx_w_calc);
     const int nt_prop2 = sh.nt_prop2, nt_taper = sh.nt_taper;
     const int nsnap = (nt_prop2 - 1) / j.store_snap;
     const size_t fstride = sl.s.g.field_cells();
@@ -1575,11 +1578,183 @@ int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
         TRY(e->get(("args" + tag).c_str(), abytes, (void**)&sl.d_args));
         CUDA_TRY(cudaMemcpyAsync(sl.d_args, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
     }
+    sl.ops.clear();
+    for (int q = 0; q < sl.nfwd; ++q) sl.ops.push_back(SlotOp{OP_LAUNCH, 0, q, sl.tiles[0], nullptr});
+    if (mixed) {
+        std::vector<int> ms = sl.pairs ? sl.pend : std::vector<int>{sl.pending};
+        for (int m : ms)
+            if (m > 0) sl.ops.push_back(SlotOp{OP_QUANT, 0, m, 0, sl.mb.snap16 + (size_t)(m - 1) * fstride});
+    }
+    sl.ops.push_back(SlotOp{OP_RESET, 0, 0, 0, nullptr});  // second propagator call: fresh wavefield
+    for (int q = 0; q < sl.nbwd; ++q)
+        sl.ops.push_back(SlotOp{OP_LAUNCH, sl.bwd_mode, sl.nfwd + q, sl.tiles[1], nullptr});
+    return PSDM_OK;
+}
+
+// The program of a checkpointed slot's shot (FP32 or mixed precision): a
+// forward pass on the slot's second state `f` without snapshots, saving
+// the state every K steps; then the backward pass, before whose first
+// imaging step of each segment of K forward steps (last segment first) the
+// segment is recomputed from its checkpoint with its snapshots, into K
+// FP32 slots or K/ks + 2 reused 16-bit slots.  The recomputed snapshots are
+// those of the uncheckpointed pass bit for bit, so is the image.
+int batch_program_ckpt(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i, const WinGeom& w, const float* d_vp,
+                       const float* d_tgt, int K) {
+    const psdm_shot& sh = j.shots[i];
+    const std::string& tag = sl.tag;
+    const int nt_prop2 = sh.nt_prop2, nt_taper = sh.nt_taper, ks = j.store_snap;
+    const int nsnap = (nt_prop2 - 1) / ks;
+    const size_t fstride = sl.s.g.field_cells();
+    const bool mixed = j.prm->precision != PSDM_PREC_FP32;
+    const int nsteps = nt_prop2 - 1, nseg = (nsteps + K - 1) / K;
+    TRY(setup_shot(e, j.prm, j.ny, sh.nx_w, j.dd, j.dt, d_vp, &sl.f, tag + "_ckf"));
+    const size_t sf = state_floats(sl.f);
+    sl.ckpts = nullptr;
+    if (nseg > 1) TRY(e->get(("ck_states" + tag).c_str(), sf * (size_t)(nseg - 1), &sl.ckpts));
+    TRY(e->get(("imgp" + tag).c_str(), fstride, &sl.d_imgp));
+    const int S = K / ks + 2;  // 16-bit slots of one segment, reused segment after segment
+    float* segbuf = nullptr;
+    if (mixed)
+        TRY(mixed_bufs(e, sl.s, j.prm->precision, ks, nt_prop2, tag, &sl.mb, S));
+    else
+        TRY(e->get(("ck_segment" + tag).c_str(), fstride * (size_t)K, &segbuf));
+    const std::vector<float> wts = taper_weights(nt_prop2, nt_taper, j.taper_option, j.N_taper, j.N_zeros);
+    // Arguments: [0, nsteps) the first forward pass, [nsteps, 2 nsteps) the
+    // recomputation of each step, then the backward steps.
+    std::vector<StepArgs> steps;
+    TRY(build_forward(e, sl.f, nt_prop2, ks, j.d_S, w.zs, w.xs, nullptr, 0, 0, nullptr, nullptr, tag + "_ckf", &steps,
+                      true));
+    for (int t = 0; t < nsteps; ++t) steps.push_back(steps[t]);
+    std::vector<int> seg_pending(nseg, 0);  // mixed: the snapshot staged by a segment's last step
+    for (int jj = 0; jj < nseg; ++jj) {
+        int prev = 0;
+        for (int t = jj * K; t < std::min((jj + 1) * K, nsteps); ++t) {
+            StepArgs& a = steps[(size_t)nsteps + t];
+            const int k = t + 2;
+            const bool snap = (k - 1) % ks == 0 && (k - 1) / ks >= 1 && (k - 1) / ks <= nsnap;
+            if (!mixed) {
+                if (snap) a.field = segbuf + (size_t)(t % K) * fstride;
+                continue;
+            }
+            a.kind16 = sl.mb.kind;
+            a.field = nullptr;
+            a.field_amax = nullptr;
+            a.q_src = nullptr;
+            if (prev > 0) {  // convert the snapshot staged by the previous step
+                a.q_src = sl.mb.stage[prev & 3];
+                a.q_amax = sl.mb.amax + (prev - 1);
+                a.q_dst = sl.mb.snap16 + (size_t)((prev - 1) % S) * fstride;
+                a.q_iscale = sl.mb.iscale + (prev - 1);
+                a.q_n = (int)fstride;
+                prev = 0;
+            }
+            if (snap) {
+                const int m = (k - 1) / ks;
+                a.field = sl.mb.stage[m & 3];
+                a.field_amax = sl.mb.amax + (m - 1);
+                prev = m;
+            }
+        }
+        seg_pending[jj] = prev;
+    }
+    const size_t b0 = steps.size();
+    std::vector<int> slot;
+    TRY(build_backward(e, sl.s, nt_taper, ks, nt_taper, d_tgt, 1, sh.NumRec, w.zr.data(), w.xr.data(),
+                       mixed ? nullptr : segbuf, 1, nsnap, wts.data(), sl.d_imgp, tag, &steps, &slot, true));
+    const int nbwd = (int)(steps.size() - b0);
+    if (mixed) {
+        mixed_backward_args(sl.mb, nt_taper, wts.data(), steps, b0);
+        for (int q = 0; q < nbwd; ++q) {  // the slot each step images, in the segment's 16-bit slots
+            StepArgs& a = steps[b0 + q];
+            slot[q] = 0;
+            if (a.field16 == nullptr) continue;
+            const int m = (int)(a.field_iscale - sl.mb.iscale) + 1;
+            slot[q] = m;
+            a.field16 = sl.mb.snap16 + (size_t)((m - 1) % S) * fstride;
+        }
+    } else {
+        for (int q = 0; q < nbwd; ++q)
+            if (slot[q] > 0) steps[b0 + q].field = segbuf + (size_t)((ks * slot[q] - 1) % K) * fstride;
+    }
+    const int ftiles = nsteps > 0 ? steps[0].r_first[steps[0].nrect] : 0;
+    const int btiles = nbwd > 0 ? steps[b0].r_first[steps[b0].nrect] : 0;
+    sl.pairs = false;
+    sl.bwd_mode = mixed ? 2 : 1;
+    sl.ops.clear();
+    for (int t = 0; t < nsteps; ++t) {
+        if (t > 0 && t % K == 0) sl.ops.push_back(SlotOp{OP_SAVE, 0, t / K - 1, 0, nullptr});
+        sl.ops.push_back(SlotOp{OP_LAUNCH, 0, t, ftiles, nullptr});
+    }
+    int cur = -1, recomputed = 0;
+    for (int q = 0; q < nbwd; ++q) {
+        const int m = slot[q];
+        if (m > 0) {
+            const int jj = (ks * m - 1) / K;  // segment of forward step t = ks*m - 1
+            if (jj != cur) {
+                sl.ops.push_back(jj == 0 ? SlotOp{OP_RESET_F, 0, 0, 0, nullptr}
+                                         : SlotOp{OP_RESTORE, 0, jj - 1, 0, nullptr});
+                const int t1 = std::min((jj + 1) * K, nsteps);
+                for (int t = jj * K; t < t1; ++t) sl.ops.push_back(SlotOp{OP_LAUNCH, 0, nsteps + t, ftiles, nullptr});
+                recomputed += t1 - jj * K;
+                const int pm = seg_pending[jj];
+                if (mixed && pm > 0)
+                    sl.ops.push_back(SlotOp{OP_QUANT, 0, pm, 0, sl.mb.snap16 + (size_t)((pm - 1) % S) * fstride});
+                cur = jj;
+            }
+        }
+        sl.ops.push_back(SlotOp{OP_LAUNCH, sl.bwd_mode, (int)b0 + q, btiles, nullptr});
+    }
+    sl.nfwd = nsteps;
+    sl.nbwd = nbwd;
+    sl.fwd_steps = nsteps + recomputed;
+    sl.bwd_steps = nbwd;
+    const size_t abytes = steps.size() * sizeof(StepArgs);
+    StepArgs* h_args = nullptr;
+    TRY(e->get_pinned(("hargs" + tag).c_str(), abytes, (void**)&h_args));
+    std::memcpy(h_args, steps.data(), abytes);
+    TRY(e->get(("args" + tag).c_str(), abytes, (void**)&sl.d_args));
+    CUDA_TRY(cudaMemcpyAsync(sl.d_args, h_args, abytes, cudaMemcpyHostToDevice, e->stream));
+    return PSDM_OK;
+}
+
+int batch_start(psdm_engine* e, const BatchJob& j, BatchSlot& sl, int i) {
+    const psdm_shot& sh = j.shots[i];
+    const int ny = j.ny, nx_w = sh.nx_w;
+    const std::string& tag = sl.tag;
+    const float* d_vp = sh.Vp_w;
+    const float* d_tgt = sh.Data_target;
+    const size_t nvp = (size_t)ny * nx_w, ntgt = (size_t)sh.NumRec * sh.nt_taper;
+    // The slot's page-locked staging is reused only once its previous
+    // copies have completed.
+    CUDA_TRY(cudaEventSynchronize(sl.staged));
+    if (j.host_io) {
+        float *h_vp = nullptr, *h_tgt = nullptr, *dv = nullptr, *dtg = nullptr;
+        TRY(e->get_pinned(("hvp" + tag).c_str(), nvp * sizeof(float), (void**)&h_vp));
+        TRY(e->get_pinned(("htgt" + tag).c_str(), ntgt * sizeof(float), (void**)&h_tgt));
+        std::memcpy(h_vp, sh.Vp_w, nvp * sizeof(float));
+        std::memcpy(h_tgt, sh.Data_target, ntgt * sizeof(float));
+        TRY(e->get(("vp" + tag).c_str(), nvp, &dv));
+        TRY(e->get(("tgt" + tag).c_str(), ntgt, &dtg));
+        CUDA_TRY(cudaMemcpyAsync(dv, h_vp, nvp * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(dtg, h_tgt, ntgt * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        d_vp = dv;
+        d_tgt = dtg;
+    }
+    TRY(setup_shot(e, j.prm, ny, nx_w, j.dd, j.dt, d_vp, &sl.s, tag));
+    WinGeom w;
+    TRY(window_geometry(sl.s.g, sh.NumRec, sh.nxSou, sh.nySou, sh.nxRec, sh.nyRec, j.dd, j.nx, j.added_space, &w));
+    if (w.nx_w_calc != nx_w)
+        return fail(PSDM_ERR_ARG, "shot %d: nx_w=%d does not match the window of its geometry (%d)", i, nx_w,
+                    w.nx_w_calc);
+    if (e->ckpt_interval > 0)
+        TRY(batch_program_ckpt(e, j, sl, i, w, d_vp, d_tgt, e->ckpt_interval));
+    else
+        TRY(batch_program_plain(e, j, sl, i, w, d_tgt));
+    const size_t fstride = sl.s.g.field_cells();
     CUDA_TRY(cudaEventRecord(sl.staged, e->stream));
     CUDA_TRY(cudaMemsetAsync(sl.d_imgp, 0, fstride * sizeof(float), e->stream));
     sl.shot = i;
-    sl.pass = sl.nfwd > 0 ? 0 : 1;
-    sl.k = 0;
+    sl.pc = 0;
     sl.out_ny = ny;
     sl.out_nx = nx_w;
     sl.d_out = j.host_io ? nullptr : sh.PSDM_w;
@@ -1628,10 +1803,20 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         TRY(build_grid(j.prm, j.ny, j.shots[i].nx_w, &g));
         const size_t nsnap = (size_t)(j.shots[i].nt_prop2 - 1) / j.store_snap;
         const size_t steps = (size_t)j.shots[i].nt_prop2 + j.shots[i].nt_taper;
-        const size_t snap_bytes = j.prm->precision != PSDM_PREC_FP32
-                                      ? (nsnap * 2 + 6 * 4) * g.field_cells()   // 16-bit slots, 4 stages, comp, image
-                                      : (nsnap + 1) * g.field_cells() * sizeof(float);
-        size_t b = 13 * g.cells() * sizeof(float) + snap_bytes + steps * sizeof(PairArgs);
+        const bool mixed = j.prm->precision != PSDM_PREC_FP32;
+        const int K = e->ckpt_interval;
+        size_t b;
+        if (K > 0) {  // two states, the checkpoints, one segment's snapshots
+            const size_t nsteps = (size_t)j.shots[i].nt_prop2 - 1, nseg = (nsteps + K - 1) / K;
+            const size_t seg = mixed ? ((size_t)(K / j.store_snap + 2) * 2 + 6 * 4) * g.field_cells()
+                                     : ((size_t)K + 1) * g.field_cells() * sizeof(float);
+            b = 2 * 13 * g.cells() * sizeof(float) + (nseg - 1) * (8 * g.cells() + 2 * (size_t)g.nxt) * sizeof(float) +
+                seg + (nsteps + steps) * sizeof(PairArgs);
+        } else {
+            const size_t snap_bytes = mixed ? (nsnap * 2 + 6 * 4) * g.field_cells()  // 16-bit slots, 4 stages, comp, image
+                                            : (nsnap + 1) * g.field_cells() * sizeof(float);
+            b = 13 * g.cells() * sizeof(float) + snap_bytes + steps * sizeof(PairArgs);
+        }
         if (j.host_io) b += ((size_t)j.ny * j.shots[i].nx_w + (size_t)j.shots[i].NumRec * j.shots[i].nt_taper) *
                             sizeof(float);
         per_slot = std::max(per_slot, b);
@@ -1675,8 +1860,50 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
     }
     int next = 0;
     for (int k = 0; rc == PSDM_OK && k < nslots && next < j.nshots; ++k) rc = batch_start(e, j, slots[k], next++);
+    // Run a slot's program up to its next launch; a finished shot hands over
+    // its image and the slot takes the next shot.
+    auto advance = [&](BatchSlot& sl) -> int {
+        for (;;) {
+            if (sl.shot < 0) return PSDM_OK;
+            if (sl.pc >= sl.ops.size()) {
+                e->fwd_steps += sl.fwd_steps;
+                e->bwd_steps += sl.bwd_steps;
+                TRY(batch_finish(e, j, sl));
+                sl.shot = -1;
+                if (next < j.nshots) {
+                    TRY(batch_flush(e, sl));
+                    TRY(batch_start(e, j, sl, next++));
+                }
+                continue;
+            }
+            const SlotOp& op = sl.ops[sl.pc];
+            if (op.kind == OP_LAUNCH) return PSDM_OK;
+            switch (op.kind) {
+                case OP_SAVE:
+                    TRY(copy_state(e, sl.f, sl.ckpts + state_floats(sl.f) * (size_t)op.arg, true));
+                    break;
+                case OP_RESTORE:
+                    TRY(copy_state(e, sl.f, sl.ckpts + state_floats(sl.f) * (size_t)op.arg, false));
+                    break;
+                case OP_RESET: TRY(reset_state(e, &sl.s)); break;
+                case OP_RESET_F: TRY(reset_state(e, &sl.f)); break;
+                default: {  // OP_QUANT
+                    const int m = op.arg;
+                    const int qr = launch_quantize(sl.mb.stage[m & 3], sl.mb.amax + (m - 1), op.dst,
+                                                   sl.mb.iscale + (m - 1), (int)sl.mb.fstride, sl.mb.kind, e->stream);
+                    if (qr) return fail(PSDM_ERR_CUDA, "snapshot conversion launch: %s",
+                                        cudaGetErrorString((cudaError_t)qr));
+                    e->launches += 1;
+                }
+            }
+            ++sl.pc;
+        }
+    };
     int sel = 0;
     while (rc == PSDM_OK) {
+        for (BatchSlot& sl : slots)
+            if (rc == PSDM_OK) rc = advance(sl);
+        if (rc != PSDM_OK) break;
         BatchParams bp;
         PairBatchParams pb;
         std::memset(&bp, 0, sizeof(bp));
@@ -1685,15 +1912,14 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         bool pairs = false;
         for (BatchSlot& sl : slots) {
             if (sl.shot < 0) continue;
+            const SlotOp& op = sl.ops[sl.pc];
             pairs = sl.pairs;  // the same for every slot of a call
-            const int md = sl.pass == 0 ? 0 : sl.bwd_mode;
-            const int at = sl.pass == 0 ? sl.k : sl.nfwd + sl.k;
-            bp.mode[n] = pb.mode[n] = md;
+            bp.mode[n] = pb.mode[n] = op.mode;
             if (sl.pairs)
-                pb.args[n] = sl.d_pargs + at;
+                pb.args[n] = sl.d_pargs + op.arg;
             else
-                bp.args[n] = sl.d_args + at;
-            bp.first[n + 1] = pb.first[n + 1] = bp.first[n] + sl.tiles[sl.pass];
+                bp.args[n] = sl.d_args + op.arg;
+            bp.first[n + 1] = pb.first[n + 1] = bp.first[n] + op.tiles;
             ++n;
         }
         if (n == 0) break;
@@ -1708,36 +1934,8 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
             break;
         }
         e->launches += 1;
-        for (BatchSlot& sl : slots) {
-            if (sl.shot < 0) continue;
-            sl.k += 1;
-            if (sl.pass == 0) {
-                if (sl.k < sl.nfwd) continue;
-                e->fwd_steps += sl.fwd_steps;
-                // Second propagator call on the same model: fresh wavefield.
-                if (sl.bwd_mode == 2) {
-                    if (sl.pairs)
-                        for (int m : sl.pend) rc = rc == PSDM_OK ? mixed_quantize(e, sl.mb, m) : rc;
-                    else
-                        rc = mixed_quantize(e, sl.mb, sl.pending);
-                }
-                if (rc == PSDM_OK) rc = reset_state(e, &sl.s);
-                sl.pass = 1;
-                sl.k = 0;
-                if (rc != PSDM_OK) break;
-                if (sl.nbwd > 0) continue;
-            } else {
-                if (sl.k < sl.nbwd) continue;
-                e->bwd_steps += sl.bwd_steps;
-            }
-            rc = batch_finish(e, j, sl);
-            sl.shot = -1;
-            if (rc == PSDM_OK && next < j.nshots) {
-                rc = batch_flush(e, sl);
-                if (rc == PSDM_OK) rc = batch_start(e, j, sl, next++);
-            }
-            if (rc != PSDM_OK) break;
-        }
+        for (BatchSlot& sl : slots)
+            if (sl.shot >= 0) ++sl.pc;
     }
     for (BatchSlot& sl : slots) {
         if (rc == PSDM_OK) rc = batch_flush(e, sl);
@@ -1746,6 +1944,20 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
             cudaEventDestroy(sl.staged);
         }
     }
+    return rc;
+}
+
+// One mixed-precision shot with checkpoints: the batched engine's
+// checkpointed program in one slot.
+int rtm_shot_mixed_ckpt(psdm_engine* e, const psdm_params* prm, int NumRec, int nxSou, int nySou, const int* nxRec,
+                        const int* nyRec, const float* d_S, const float* d_tgt, float dd, float dt, int ny, int nx,
+                        int nx_w, const float* d_vp, float added_space, int store_snap, int nt_prop2, int nt_taper,
+                        int taper_option, int N_taper, int N_zeros, float* d_img) {
+    psdm_shot sh{NumRec, nxSou, nySou, nxRec, nyRec, nx_w, nt_prop2, nt_taper, d_vp, d_tgt, d_img};
+    BatchJob j{prm, &sh, 1, d_S, dd, dt, added_space, ny, nx, store_snap, taper_option, N_taper, N_zeros, false};
+    const int slots = e->batch_slots;
+    const int rc = run_batch(e, j, 1);
+    e->batch_slots = slots;
     return rc;
 }
 
@@ -2047,34 +2259,29 @@ int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t n
     const double base = 13.0 * cells * 4 + field * 4 + (double)(nt_prop2 + nt_taper) / 2 * sizeof(PairArgs) +
                         ((double)ny * nx_w + (double)NumRec * nt_taper + nt_prop2) * 4;
     const int mslots = std::min(max_slots > 0 ? (int)max_slots : kMaxSlots, kMaxSlots);
-    if (prm->precision != PSDM_PREC_FP32) {
-        // 16-bit snapshots, four FP32 staging buffers and the Kahan compensation
-        const double per = base + (double)nsnap * field * 2 + 5.0 * field * 4;
-        out->bytes_per_slot = (int64_t)per;
-        const double n = avail > 0 ? std::floor(avail / per) : 0.0;
-        out->slots = (int)std::min<double>(n, mslots);
-        out->fits = out->slots >= 1;
-        if (!out->fits)
-            return fail(PSDM_ERR_NOMEM, "one mixed-precision shot needs %.2f GB, the budget leaves %.2f GB",
-                        per / 1e9, avail / 1e9);
-        return PSDM_OK;
-    }
-    const double all = base + (double)nsnap * field * 4;
+    const bool mixed = prm->precision != PSDM_PREC_FP32;
+    auto slots_of = [&](double per) { return (int)std::min<double>(avail > 0 ? std::floor(avail / per) : 0.0, mslots); };
+    // All snapshots: 16-bit slots with four FP32 staging buffers and the
+    // Kahan compensation, or FP32 slots.
+    const double all = mixed ? base + (double)nsnap * field * 2 + 5.0 * field * 4 : base + (double)nsnap * field * 4;
     if (all <= avail) {
         out->bytes_per_slot = (int64_t)all;
-        out->slots = (int)std::min<double>(std::floor(avail / all), mslots);
+        out->slots = slots_of(all);
         out->fits = 1;
         return PSDM_OK;
     }
     // Checkpoints every K steps: the state (8 grids and two history rows) at
-    // each segment start but the first, a K-slot snapshot buffer, and the
-    // recomputing shot's own grids; the memory is smallest near
-    // K = sqrt(steps * state / snapshot).
+    // each segment start but the first, one segment's snapshots (K FP32
+    // slots, or K/ks + 2 16-bit slots with the staging buffers), and the
+    // recomputing state's own grids; the memory is smallest near
+    // K = sqrt(steps * state / snapshot).  The recomputation costs one more
+    // forward pass whatever K is.
     const int nsteps = nt_prop2 - 1;
     const double state = (8.0 * cells + 2.0 * g.nxt) * 4;
     auto mem = [&](int K) {
         const int nseg = (nsteps + K - 1) / K;
-        return base + 13.0 * cells * 4 + (double)K * field * 4 + (double)(nseg - 1) * state;
+        const double seg = mixed ? (double)(K / store_snap + 2) * field * 2 + 5.0 * field * 4 : (double)K * field * 4;
+        return base + 13.0 * cells * 4 + seg + (double)(nseg - 1) * state;
     };
     int best = 1;
     for (int K = 1; K <= nsteps; ++K)
@@ -2082,10 +2289,10 @@ int psdm_plan_memory(const psdm_params* prm, int32_t ny, int32_t nx_w, int32_t n
     best = std::max(best, std::min(16, nsteps));  // at most one state copy per 16 steps
     out->bytes_per_slot = (int64_t)mem(best);
     if (mem(best) > avail)
-        return fail(PSDM_ERR_NOMEM, "one FP32 shot needs %.2f GB even with checkpoints every %d steps, the budget "
-                    "leaves %.2f GB", mem(best) / 1e9, best, avail / 1e9);
+        return fail(PSDM_ERR_NOMEM, "one %s shot needs %.2f GB even with checkpoints every %d steps, the budget "
+                    "leaves %.2f GB", mixed ? "mixed-precision" : "FP32", mem(best) / 1e9, best, avail / 1e9);
     out->checkpoint_interval = best;
-    out->slots = 1;
+    out->slots = slots_of(mem(best));
     out->fits = 1;
     return PSDM_OK;
 }
