@@ -98,6 +98,7 @@ struct psdm_engine {
     cudaEvent_t pass_staged[3] = {nullptr, nullptr, nullptr};  // copies out of the staging buffers done
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: shots keep checkpoints every K steps instead of all snapshots
+    std::map<int, cudaGraphExec_t> bgraphs;  // batched launches: an executable graph per run length
     bool recon = false;     // FP32 shots reconstruct the source wavefield from a saved band
     std::map<std::pair<int, int>, std::array<int, 2>> fft_plans;  // (length, batch) -> cuFFT plans
     // dt -> (fast division exact, 1/dt, lo, hi); the check costs ~50 ms
@@ -160,6 +161,9 @@ struct psdm_engine {
         return PSDM_OK;
     }
     void drop_graphs() {
+        for (auto& kv : bgraphs)
+            if (kv.second) cudaGraphExecDestroy(kv.second);
+        bgraphs.clear();
         for (auto& g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
             g.exec = nullptr;
@@ -1899,8 +1903,69 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
             ++sl.pc;
         }
     };
+    // The time loop is captured in CUDA graphs: the launches between two host
+    // operations of any slot are queued and replayed as graphs of up to
+    // kBatchRun launches (an executable graph per run length, updated in
+    // place with the run's parameters).
+    struct Queued {
+        bool pairs;
+        BatchParams bp;
+        PairBatchParams pb;
+    };
+    constexpr int kBatchRun = 64;
+    std::vector<Queued> queued;
+    auto launch_one = [&](const Queued& q, cudaStream_t st) {
+        return q.pairs ? launch_pair_batch(q.pb, e->num_sms, st) : launch_batch_step(q.bp, e->num_sms, st);
+    };
+    auto flush = [&]() -> int {
+        if (queued.empty()) return PSDM_OK;
+        bool done = false;
+        if (e->use_graphs && queued.size() >= 8) {
+            cudaStream_t cs = e->own_stream;
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                for (const Queued& q : queued)
+                    if (launch_one(q, cs) != 0) {
+                        ok = false;
+                        break;
+                    }
+                ok = (cudaStreamEndCapture(cs, &graph) == cudaSuccess) && ok;
+            }
+            cudaGraphExec_t& ex = e->bgraphs[(int)queued.size()];
+            if (ok && ex) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(ex, graph, &info) != cudaSuccess) {
+                    cudaGraphExecDestroy(ex);
+                    ex = nullptr;
+                }
+            }
+            if (ok && !ex) ok = cudaGraphInstantiate(&ex, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();  // clear a failed capture or update
+            if (ok) {
+                CUDA_TRY(cudaGraphLaunch(ex, e->stream));
+                done = true;
+            } else {
+                if (ex) cudaGraphExecDestroy(ex);
+                e->bgraphs.erase((int)queued.size());
+                e->use_graphs = false;
+            }
+        }
+        if (!done)
+            for (const Queued& q : queued) {
+                const int lr = launch_one(q, e->stream);
+                if (lr) return fail(PSDM_ERR_CUDA, "batched step launch: %s", cudaGetErrorString((cudaError_t)lr));
+            }
+        queued.clear();
+        return PSDM_OK;
+    };
     int sel = 0;
     while (rc == PSDM_OK) {
+        bool host_op = false;  // a slot is due for a state operation, or done
+        for (BatchSlot& sl : slots)
+            host_op = host_op || (sl.shot >= 0 && (sl.pc >= sl.ops.size() || sl.ops[sl.pc].kind != OP_LAUNCH));
+        if (host_op) rc = flush();
         for (BatchSlot& sl : slots)
             if (rc == PSDM_OK) rc = advance(sl);
         if (rc != PSDM_OK) break;
@@ -1927,16 +1992,13 @@ int run_batch(psdm_engine* e, const BatchJob& j, int max_slots) {
         bp.counter = pb.counter = counters;
         bp.counter_sel = pb.counter_sel = sel;
         sel ^= 1;
-        const int lr = pairs ? launch_pair_batch(pb, e->num_sms, e->stream)
-                             : launch_batch_step(bp, e->num_sms, e->stream);
-        if (lr) {
-            rc = fail(PSDM_ERR_CUDA, "batched step launch: %s", cudaGetErrorString((cudaError_t)lr));
-            break;
-        }
+        queued.push_back(Queued{pairs, bp, pb});
+        if ((int)queued.size() == kBatchRun) rc = flush();
         e->launches += 1;
         for (BatchSlot& sl : slots)
             if (sl.shot >= 0) ++sl.pc;
     }
+    if (rc == PSDM_OK) rc = flush();
     for (BatchSlot& sl : slots) {
         if (rc == PSDM_OK) rc = batch_flush(e, sl);
         if (sl.staged) {
