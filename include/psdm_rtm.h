@@ -33,7 +33,13 @@ enum {
     PSDM_ERR_STATE = -4  /* engine misuse (null engine, ...) */
 };
 
-/* Snapshot storage precision of the engine (psdm_params.precision). */
+/*
+ * Snapshot storage precision of the engine (psdm_params.precision).  The
+ * 16-bit forms propagate in FP32, keep an FP32 image with Kahan compensation,
+ * and set up their FD coefficients and C-PML profiles in double precision,
+ * rounded once to FP32; PSDM_PREC_FP32 keeps the reference's single-precision
+ * set-up (src/solver_FD_coeffs.f90, src/solver_PML_coeffs.f90).
+ */
 enum {
     PSDM_PREC_FP32 = 0,  /* plain FP32: the reference's arithmetic, bit for bit */
     PSDM_PREC_FP16 = 1,  /* FP16 snapshots with per-snapshot power-of-two scale */

@@ -319,10 +319,14 @@ void scatter(Arr2<T>& p3, const Strip<T>& s, const std::vector<int>& vy, const s
 //     power of two 2^k chosen from the snapshot's largest magnitude A so that
 //     A*2^k lies in [2^14, 2^15); read back as float(h) * 2^-k;
 //   kahan: the image is summed with compensated (Kahan) summation.
+//   coef64: the float build takes its FD coefficients and C-PML profiles
+//     from the double-precision set-up, rounded once (the engine's set-up of
+//     the form).
 struct MixedOpts {
     int pair_mode = 0;
     int q16 = 0;
     int kahan = 0;
+    int coef64 = 0;
 };
 
 // x rounded to the nearest binary16 (mant = 10, emin = -14) or bfloat16
@@ -460,6 +464,20 @@ void solver_ac(int iprop, int disk_mode, int dPML, int fs, int NumRec,
     int snap = (iprop == 1) ? 0 : nt_snap;
     fd_coef<T>(1, acc, coef1.data());
     fd_coef<T>(2, acc, coef2.data());
+    if (mo && mo->coef64 && sizeof(T) == sizeof(float)) {
+        std::vector<double> a64(dn, 0.0), b64(dn, 0.0), c1(acc + 1), c2(acc + 1);
+        Arr2<double> t[8] = {Arr2<double>(dn, dn), Arr2<double>(dn, dn), Arr2<double>(dn, dn), Arr2<double>(dn, dn),
+                             Arr2<double>(dn, dn), Arr2<double>(dn, dn), Arr2<double>(dn, dn), Arr2<double>(dn, dn)};
+        pml_coeffs<double>(acc, dPML, double(dt), double(dmodel), dn, a64.data(), b64.data(), t[0], t[1], t[2], t[3],
+                           t[4], t[5], t[6], t[7]);
+        Arr2<T>* dst[8] = {&ldA, &rdA, &luA, &ruA, &ldB, &rdB, &luB, &ruB};
+        for (int q = 0; q < 8; ++q)
+            for (size_t i = 0; i < dst[q]->v.size(); ++i) dst[q]->v[i] = T(t[q].v[i]);
+        for (int i = 0; i < dn; ++i) { fA[i] = T(a64[i]); fB[i] = T(b64[i]); }
+        fd_coef<double>(1, acc, c1.data());
+        fd_coef<double>(2, acc, c2.data());
+        for (int k = 0; k <= acc; ++k) { coef1[k] = T(c1[k]); coef2[k] = T(c2[k]); }
+    }
 
     if (iprop == 1)
         for (size_t q = 0; q < (size_t)nt * NumRec; ++q) out[q] = T(0);
@@ -803,6 +821,7 @@ void orc_rtm_shot_mixed_f(int q16, int kahan, int disk_mode, int dPML, int fs, i
     mo.pair_mode = 1;
     mo.q16 = q16;
     mo.kahan = kahan;
+    mo.coef64 = q16 != 0;  // the engine's 16-bit forms; q16 = 0 keeps the reference's set-up
     rtm_shot_mixed<float>(mo, disk_mode, dPML, fs, NumRec, nxSou, nySou, nxRec, nyRec, Data_source, Data_target, dd,
                           dt, ny, nx, nx_w, Vp_w, added_space, store_snap, nt_prop2, nt_taper, taper_option, N_taper,
                           N_zeros, PSDM_w, Fields_out);

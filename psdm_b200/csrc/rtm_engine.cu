@@ -289,9 +289,25 @@ int setup_shot(psdm_engine* e, const psdm_params* prm, int ny, int nx, float dd,
     s->err = e->d_err;
 
     std::vector<float> fA(g.dn), fB(g.dn);
-    pml_profiles_f32(kAcc, g.dPML, dt, dd, g.dn, fA.data(), fB.data());
-    psdm_fd_coef(1, kAcc, s->cf1);
-    psdm_fd_coef(2, kAcc, s->cf2);
+    if (prm->precision == PSDM_PREC_FP32) {  // the reference's single-precision set-up
+        pml_profiles_f32(kAcc, g.dPML, dt, dd, g.dn, fA.data(), fB.data());
+        psdm_fd_coef(1, kAcc, s->cf1);
+        psdm_fd_coef(2, kAcc, s->cf2);
+    } else {  // mixed precision: FD coefficients and C-PML profiles in double, rounded once
+        std::vector<double> a64(g.dn), b64(g.dn);
+        pml_profiles_f64(kAcc, g.dPML, (double)dt, (double)dd, g.dn, a64.data(), b64.data());
+        for (int i = 0; i < g.dn; ++i) {
+            fA[i] = (float)a64[i];
+            fB[i] = (float)b64[i];
+        }
+        double c1[4], c2[4];
+        fd_coef_f64(1, c1);
+        fd_coef_f64(2, c2);
+        for (int k = 0; k < 4; ++k) {
+            s->cf1[k] = (float)c1[k];
+            s->cf2[k] = (float)c2[k];
+        }
+    }
     auto it = e->div_cache.find(dt);
     if (it == e->div_cache.end()) {
         float r = 0.f, lo = 0.f, hi = 0.f, tiny = 0.f;

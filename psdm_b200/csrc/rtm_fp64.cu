@@ -193,16 +193,6 @@ __global__ void widen_kernel(const float* in, double* out, size_t n) {
         out[i] = (double)in[i];
 }
 
-// FD coefficients of src/solver_FD_coeffs.f90:14-19,43-50,68 (acc = 3) as
-// double-precision rationals; the centre tap of the 2nd derivative halved.
-void fd_coef_f64(int num, double* c) {
-    if (num == 1) {
-        c[0] = 0.0; c[1] = 3.0 / 4.0; c[2] = -3.0 / 20.0; c[3] = 1.0 / 60.0;
-    } else {
-        c[0] = (-49.0 / 18.0) / 2.0; c[1] = 3.0 / 2.0; c[2] = -3.0 / 20.0; c[3] = 1.0 / 90.0;
-    }
-}
-
 // Device buffers of one FP64 shot, freed on scope exit.
 struct Dev64 {
     std::vector<void*> ptrs;

@@ -42,6 +42,16 @@ void pml_profiles_f32(int acc, int dPML, float dt, float d, int dn, float* fA, f
     for (int i = dPML + acc + 1; i <= dn; ++i) { fA[i - 1] = fA[dPML + acc - 1]; fB[i - 1] = fB[dPML + acc - 1]; }
 }
 
+// FD coefficients of src/solver_FD_coeffs.f90:14-19,43-50,68 (acc = 3) as
+// double-precision rationals; the centre tap of the 2nd derivative halved.
+void fd_coef_f64(int num, double* c) {
+    if (num == 1) {
+        c[0] = 0.0; c[1] = 3.0 / 4.0; c[2] = -3.0 / 20.0; c[3] = 1.0 / 60.0;
+    } else {
+        c[0] = (-49.0 / 18.0) / 2.0; c[1] = 3.0 / 2.0; c[2] = -3.0 / 20.0; c[3] = 1.0 / 90.0;
+    }
+}
+
 void pml_profiles_f64(int acc, int dPML, double dt, double d, int dn, double* fA, double* fB) {
     for (int i = 0; i < dn; ++i) { fA[i] = 0.0; fB[i] = 0.0; }
     const double pi = 3.14159265;

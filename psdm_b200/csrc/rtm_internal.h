@@ -13,6 +13,7 @@ constexpr int kAcc = 3;  // FD half-width (acc=3, src/solver_ac_forward_ram.f90:
 
 void pml_profiles_f32(int acc, int dPML, float dt, float d, int dn, float* fA, float* fB);
 void pml_profiles_f64(int acc, int dPML, double dt, double d, int dn, double* fA, double* fB);
+void fd_coef_f64(int num, double* c);  // acc = 3
 float taper_weight(int n, int N_taper);
 // True if x/y may be computed as RN(q0 + (x - q0*y)*r), q0 = RN(x*r),
 // r = RN(1/y), for |x| in [lo, hi] (exhaustive check over one binade).

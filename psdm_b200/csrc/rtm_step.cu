@@ -227,7 +227,10 @@ __device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __r
 // instructions (per-element rounding of the scalar ones); adds that consume
 // a product stay scalar so that no multiply-add is ever fused.
 // Returns false if the copies did not complete (error reported).
-template <int MODE, int XS>
+// ST: p1 and c2 of the tile are copied into shared memory with p (batched
+// launches, whose operands come from HBM rather than L2: every load of the
+// tile is in flight at once), instead of being read one column ahead.
+template <int MODE, int XS, bool ST = false>
 __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int r,
                                               int t) {
     constexpr int TX = tile_cols(XS);
@@ -243,14 +246,22 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     const int sz0 = z0 - 4, sx0 = x0 - 3;
     const int dn = a.dn;
     float* ps = sm;                  // p, (ncols+6) columns of HZ rows
+    float* pms = ps + tile_smem_cols(XS) * HZ;  // ST: p1, then c2, ncols columns of TZ rows each
+    float* c2s = pms + tile_cols(XS) * TZ;
     if (wy == 0) {
-        const uint32_t prow = (uint32_t)(nrows + 8) * 4u;
-        const uint32_t bytes = (uint32_t)(ncols + 6) * prow;
+        const uint32_t prow = (uint32_t)(nrows + 8) * 4u, trow = (uint32_t)nrows * 4u;
+        const uint32_t bytes = (uint32_t)(ncols + 6) * prow + (ST ? (uint32_t)ncols * trow * 2u : 0u);
         fence_proxy_async();  // the previous tile's shared reads precede these writes
         if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
         __syncwarp();
         for (int c = lane; c < ncols + 6; c += 32)
             bulk_g2s(ps + c * HZ, a.p + (sx0 + c) * a.ldz + sz0, prow, bar);
+        if (ST)
+            for (int c = lane; c < ncols; c += 32) {
+                const int gc = (x0 + c) * a.ldz + z0;
+                bulk_g2s(pms + c * TZ, a.pm + gc, trow, bar);
+                bulk_g2s(c2s + c * TZ, a.c2 + gc, trow, bar);
+            }
     }
     const int q = 4 * lane;        // first tile row of this thread's float4
     const int c0 = wy * XS;        // first tile column of this thread
@@ -278,7 +289,7 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     float* __restrict__ pmp = a.pm;
     int g = (x0 + c0) * a.ldz + zd;
     float4 pmN = make_float4(0.f, 0.f, 0.f, 0.f), c2N = pmN;
-    if (active) {
+    if (active && !ST) {
         pmN = *reinterpret_cast<const float4*>(pmp + g);
         c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
     }
@@ -306,8 +317,11 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         win[6] = ps4[(col + 6) * HQ + qr];
         const float4 zm = ps4[(col + 3) * HQ + qr - 1];
         const float4 zp = ps4[(col + 3) * HQ + qr + 1];
-        const float4 pmv = pmN, c2v = c2N;
-        if (c + 1 < ncol) {
+        float4 pmv = pmN, c2v = c2N;
+        if (ST) {
+            pmv = *reinterpret_cast<const float4*>(pms + col * TZ + q);
+            c2v = *reinterpret_cast<const float4*>(c2s + col * TZ + q);
+        } else if (c + 1 < ncol) {
             pmN = *reinterpret_cast<const float4*>(pmp + g + a.ldz);
             c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g + a.ldz));
         }
@@ -660,13 +674,22 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
 
 // One tile (block-local index b of the step described by `a`).  Returns
 // false if its bulk copies did not complete.
-template <int MODE, int XS = XS_MANY>
+#ifndef PSDM_BATCH_STAGE
+#define PSDM_BATCH_STAGE 1
+#endif
+// Batched launches stage p1 and c2 of interior tiles with p (PSDM_BATCH_STAGE).
+constexpr bool kBatchStage = PSDM_BATCH_STAGE != 0;
+constexpr int batch_smem_floats() {
+    return smem_floats<XS_MANY>() + (kBatchStage ? 2 * TZ * tile_cols(XS_MANY) : 0);
+}
+
+template <int MODE, int XS = XS_MANY, bool ST = (XS == XS_MANY && kBatchStage)>
 __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int b) {
     int r = 0;
     while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
     const int t = b - a.r_first[r];
     switch (a.r_type[r]) {
-        case 0: return interior_tile<MODE, XS>(a, sm, bar, phase, r, t);
+        case 0: return interior_tile<MODE, XS, ST>(a, sm, bar, phase, r, t);
         case 1: xband_tile<MODE>(a, sm, r, t); return true;
         case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
         case 4: rowband_tile<MODE>(a, sm, r, t); return true;
@@ -997,7 +1020,7 @@ template <int FIXED>
 int batch_blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
-        const int bytes = smem_floats<XS_MANY>() * (int)sizeof(float);
+        const int bytes = batch_smem_floats() * (int)sizeof(float);
         cudaFuncSetAttribute(batch_step_kernel<FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_step_kernel<FIXED>, NT, bytes);
@@ -1149,7 +1172,7 @@ int launch_quantize(const float* src, const unsigned int* amax, void* dst, float
 template <int FIXED>
 int launch_batch(const BatchParams& bp, int num_sms, cudaStream_t stream) {
     const int total = bp.first[bp.nslots];
-    const int bytes = smem_floats<XS_MANY>() * (int)sizeof(float);
+    const int bytes = batch_smem_floats() * (int)sizeof(float);
     const dim3 grid(min(total, num_sms * batch_blocks_per_sm<FIXED>()));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;

@@ -40,6 +40,9 @@ class ImageStack:
     """
 
     def __init__(self, ny: int, nx: int, device=None, dtype=None, group=None):
+        """dtype: float32 (default) sums as the reference does
+        (calculate_PSDM_RTM.f90:493-497); float64 keeps the cross-shot stack
+        in double precision (window images are widened once)."""
         import torch
         self.torch = torch
         self.ny, self.nx = ny, nx
@@ -78,8 +81,15 @@ class ImageStack:
 
     def normalized(self) -> np.ndarray:
         """PSDM = PSDM_sum / Cov_sum where the fold is positive
-        (normalize_psdm, src/auxiliar_PSDM.f90:1-20), on the host."""
+        (normalize_psdm, src/auxiliar_PSDM.f90:1-20), on the host.  A stack
+        kept in float64 is divided in float64 and rounded once to float32."""
         from psdm_b200 import rtm
+        if self.psdm_sum.dtype == self.torch.float64:
+            s = self.psdm_sum.detach().cpu().numpy()
+            c = self.cov_sum.detach().cpu().numpy()
+            out = np.zeros(s.shape, np.float64)
+            np.divide(s, c, out=out, where=c > 0)
+            return out.astype(np.float32)
         s = self.psdm_sum.detach().to("cpu", self.torch.float32).numpy()
         c = self.cov_sum.detach().to("cpu", self.torch.float32).numpy()
         return rtm.normalize_psdm(s, c)

@@ -139,6 +139,39 @@ def test_single_process_stack_and_normalize(oracle):
     np.testing.assert_array_equal(stack.normalized(), oracle.normalize_psdm(want_psdm, want_cov))
 
 
+def test_float64_stack(oracle):
+    """The cross-shot stack kept in float64: the running sums are the float64
+    sums of the widened window images, and the image is the float64 quotient
+    rounded once."""
+    import torch
+    stack = driver.ImageStack(NY, NX, dtype=torch.float64)
+
+    def shot(ic):
+        res = fake_shot(ic)
+        if res is None:
+            return None
+        img, x_i, x_f = res
+        return torch.from_numpy(img), x_i, x_f
+
+    driver.migrate_lines(shot, 1, 6, stack)
+    psdm = np.zeros((NX, NY), np.float64)
+    cov = np.zeros((NX, NY), np.float64)
+    for ic in range(1, 7):
+        res = fake_shot(ic)
+        if res is None:
+            continue
+        img, x_i, x_f = res
+        psdm[x_i - 1:x_f] += img.astype(np.float64)
+        cov[x_i - 1:x_f] += 1.0
+    np.testing.assert_array_equal(stack.psdm_sum.numpy(), psdm)
+    np.testing.assert_array_equal(stack.cov_sum.numpy(), cov)
+    want = np.zeros_like(psdm)
+    np.divide(psdm, cov, out=want, where=cov > 0)
+    got = stack.normalized()
+    assert got.dtype == np.float32
+    np.testing.assert_array_equal(got, want.astype(np.float32))
+
+
 def test_window_outside_model_is_rejected():
     stack = driver.ImageStack(NY, NX)
     with pytest.raises(ValueError):
