@@ -675,9 +675,12 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
 // One tile (block-local index b of the step described by `a`).  Returns
 // false if its bulk copies did not complete.
 #ifndef PSDM_BATCH_STAGE
-#define PSDM_BATCH_STAGE 1
+#define PSDM_BATCH_STAGE 0
 #endif
-// Batched launches stage p1 and c2 of interior tiles with p (PSDM_BATCH_STAGE).
+// With PSDM_BATCH_STAGE=1, batched launches stage p1 and c2 of interior tiles
+// with p.  Off by default: the 52 KB tile leaves 4 blocks per SM instead of 5,
+// and on the B200 8 FP16 shots in flight ran at 5.73 against 6.32 shots/s
+// without it (config 4: 3.62 against 4.66).
 constexpr bool kBatchStage = PSDM_BATCH_STAGE != 0;
 constexpr int batch_smem_floats() {
     return smem_floats<XS_MANY>() + (kBatchStage ? 2 * TZ * tile_cols(XS_MANY) : 0);
