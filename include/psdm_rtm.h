@@ -222,9 +222,14 @@ int psdm_engine_set_reconstruction(psdm_engine* e, int32_t on);
  * Launch form of one shot's passes (psdm_rtm_shot, psdm_model_shot and their
  * device variants): 1 runs a pass whose steps allow it as one cooperative
  * launch in which each tile advances as soon as its neighbours finished the
- * previous step; 0 (default) launches one kernel per time step (replayed
- * from a CUDA graph).  Same results bit for bit.  Passes with the
- * mixed-precision snapshot conversion always use one launch per step.
+ * previous step; 2 runs each forward and plain backward pass as one
+ * cooperative launch of one block per region of the grid, each block keeping
+ * its region's wavefield in shared memory for the whole pass and exchanging
+ * only the ring with its neighbours (grids that fit the device's blocks;
+ * others fall back to one launch per step); 0 (default) launches one kernel
+ * per time step (replayed from a CUDA graph).  Same results bit for bit.
+ * Passes with the mixed-precision snapshots always use one launch per step.
+ * Values other than 0, 1 and 2 return PSDM_ERR_ARG.
  */
 int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on);
 /*

@@ -18,7 +18,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libpsdm_rtm.so")
 INCLUDE = os.path.join(os.path.dirname(PKG), "include")
 
-SOURCES = ["rtm_step.cu", "rtm_pair.cu", "rtm_fp64.cu", "rtm_engine.cu", "rtm_host.cpp", "rtm_noalloc.cu", "rtm_condition.cu", "su_io.cpp", "rtm_filter.cu", "nav.cpp"]
+SOURCES = ["rtm_step.cu", "rtm_pair.cu", "rtm_resident.cu", "rtm_fp64.cu", "rtm_engine.cu", "rtm_host.cpp", "rtm_noalloc.cu", "rtm_condition.cu", "su_io.cpp", "rtm_filter.cu", "nav.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -90,11 +90,15 @@ struct psdm_engine {
         std::vector<PairArgs> args;
         cudaGraphExec_t exec = nullptr;
     } pgraphs[3];
-    // Passes of one shot as one cooperative launch each (pass_kernel) where
-    // the pass allows it; the neighbour and receiver lists of the last plan
-    // of each pass kind stay on the device while the plan (key) is unchanged.
-    bool use_pass = false;
+    // Passes of one shot as one cooperative launch each where the pass allows
+    // it: 1 = pass_kernel (tiles re-read every step), 2 = res_kernel (regions
+    // resident in shared memory); the neighbour, receiver and work lists of
+    // the last plan of each pass kind stay on the device while the plan (key)
+    // is unchanged.
+    int use_pass = 0;
     std::vector<int> pass_key[3];  // by pass kind (mode)
+    std::vector<int> res_key[2];   // resident form, by pass kind
+    int res_nreg[2] = {0, 0}, res_sw[2] = {0, 0};
     cudaEvent_t pass_staged[3] = {nullptr, nullptr, nullptr};  // copies out of the staging buffers done
     int batch_slots = 0;  // slots used by the last batched call
     int ckpt_interval = 0;  // > 0: shots keep checkpoints every K steps instead of all snapshots
@@ -150,6 +154,7 @@ struct psdm_engine {
     int trim() {
         drop_graphs();
         for (auto& k : pass_key) k.clear();
+        for (auto& k : res_key) k.clear();
         for (auto& kv : fft_plans) destroy_fft_plans(kv.second.data());
         fft_plans.clear();
         for (auto& kv : bufs)
@@ -540,6 +545,105 @@ int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args
     return PSDM_OK;
 }
 
+// One resident launch (res_kernel) for the whole pass: forward and plain
+// backward passes of one shot whose grid fits the device's regions.  Returns
+// PSDM_OK when launched, 1 when the pass does not have the form, or an error.
+int launch_resident_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args, int nrec,
+                         const int* h_rec_cell) {
+    if (mode != 0 && mode != 1) return 1;
+    StepArgs base[2];
+    std::vector<PassVar> var;
+    if (!pass_form(args, base, &var)) return 1;
+    const StepArgs& a = base[0];
+    if (a.field16 != nullptr) return 1;
+    if (mode == 0 && a.nrec > 0 && (h_rec_cell == nullptr || nrec != a.nrec)) return 1;
+    const int msw = resident_max_sw();
+    if (msw < kResMinSide + 6) return 1;
+    std::vector<int> key = {mode == 0 ? a.nrec : 0, a.nrect, a.ldz, a.nxt, a.nyt, a.dn, a.zoff, a.fs, a.ny, a.nx};
+    key.insert(key.end(), a.r_type, a.r_type + a.nrect);
+    key.insert(key.end(), a.r_zd0, a.r_zd0 + a.nrect);
+    key.insert(key.end(), a.r_h, a.r_h + a.nrect);
+    if (mode == 0 && a.nrec > 0) key.insert(key.end(), h_rec_cell, h_rec_cell + nrec);
+    const std::string m = std::to_string(mode);
+    ResRegion* d_reg = nullptr;
+    int *d_nbr = nullptr, *d_rec = nullptr, *d_wf = nullptr, *d_items = nullptr;
+    int& nreg = e->res_nreg[mode];
+    int& sw = e->res_sw[mode];
+    if (key != e->res_key[mode]) {
+        e->res_key[mode].clear();
+        ResPlan plan;
+        int nb = resident_blocks_per_sm(mode, msw);
+        if (nb <= 0) return 1;
+        if (!plan_resident(a, nb * e->num_sms, msw, mode == 0 ? a.nrec : 0, h_rec_cell, &plan)) return 1;
+        if (resident_blocks_per_sm(mode, plan.sw) * e->num_sms < (int)plan.reg.size()) return 1;
+        TRY(e->get(("res_reg" + m).c_str(), plan.reg.size(), &d_reg));
+        TRY(e->get(("res_nbr" + m).c_str(), std::max<size_t>(plan.nbr.size(), 1), &d_nbr));
+        TRY(e->get(("res_rec" + m).c_str(), std::max<size_t>(plan.rec.size(), 1), &d_rec));
+        TRY(e->get(("res_wf" + m).c_str(), plan.warp_first.size(), &d_wf));
+        TRY(e->get(("res_items" + m).c_str(), std::max<size_t>(plan.items.size(), 2), &d_items));
+        CUDA_TRY(cudaMemcpyAsync(d_reg, plan.reg.data(), plan.reg.size() * sizeof(ResRegion), cudaMemcpyHostToDevice,
+                                 e->stream));
+        if (!plan.nbr.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_nbr, plan.nbr.data(), plan.nbr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                     e->stream));
+        if (!plan.rec.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_rec, plan.rec.data(), plan.rec.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                     e->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_wf, plan.warp_first.data(), plan.warp_first.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, e->stream));
+        if (!plan.items.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_items, plan.items.data(), plan.items.size() * sizeof(int),
+                                     cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));  // the host lists go out of scope
+        nreg = (int)plan.reg.size();
+        sw = plan.sw;
+        e->res_key[mode] = key;
+    } else {
+        TRY(e->get(("res_reg" + m).c_str(), (size_t)nreg, &d_reg));
+        TRY(e->get(("res_nbr" + m).c_str(), 1, &d_nbr));
+        TRY(e->get(("res_rec" + m).c_str(), 1, &d_rec));
+        TRY(e->get(("res_wf" + m).c_str(), 1, &d_wf));
+        TRY(e->get(("res_items" + m).c_str(), 2, &d_items));
+    }
+    StepArgs* d_base = nullptr;
+    PassVar* d_var = nullptr;
+    int* d_flags = nullptr;
+    TRY(e->get(("pass_base" + m).c_str(), 2, &d_base));
+    TRY(e->get(("pass_var" + m).c_str(), var.size(), &d_var));
+    TRY(e->get("pass_flags", (size_t)nreg + 1, &d_flags));  // + the abort word
+    const size_t sbytes = 2 * sizeof(StepArgs) + var.size() * sizeof(PassVar);
+    char* h = nullptr;
+    const std::string sname = "pass_stage" + m;
+    TRY(e->get_pinned(sname.c_str(), sbytes, reinterpret_cast<void**>(&h)));
+    cudaEvent_t& done = e->pass_staged[mode];
+    if (done == nullptr) CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventSynchronize(done));
+    std::memcpy(h, base, 2 * sizeof(StepArgs));
+    std::memcpy(h + 2 * sizeof(StepArgs), var.data(), var.size() * sizeof(PassVar));
+    CUDA_TRY(cudaMemcpyAsync(d_base, h, 2 * sizeof(StepArgs), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_var, h + 2 * sizeof(StepArgs), var.size() * sizeof(PassVar), cudaMemcpyHostToDevice,
+                             e->stream));
+    CUDA_TRY(cudaEventRecord(done, e->stream));
+    CUDA_TRY(cudaMemsetAsync(d_flags, 0, ((size_t)nreg + 1) * sizeof(int), e->stream));
+    ResParams rp{};
+    rp.base = d_base;
+    rp.var = d_var;
+    rp.nsteps = (int)var.size();
+    rp.nreg = nreg;
+    rp.sw = sw;
+    rp.reg = d_reg;
+    rp.nbr = d_nbr;
+    rp.rec = d_rec;
+    rp.warp_first = d_wf;
+    rp.items = d_items;
+    rp.flags = d_flags;
+    rp.abort = d_flags + nreg;
+    rp.err = a.err;
+    const int rc = launch_resident(mode, rp, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "resident pass launch: %s", cudaGetErrorString((cudaError_t)rc));
+    return PSDM_OK;
+}
+
 // Launch the step kernels of one pass.  The launches are captured once into
 // a CUDA graph and the graph is replayed while the argument list is
 // identical (same buffers, geometry, step count and per-step values), which
@@ -549,7 +653,8 @@ int launch_steps(psdm_engine* e, int mode, const std::vector<StepArgs>& args, in
                  const int* h_rec_cell = nullptr) {
     if (args.empty()) return PSDM_OK;
     if (e->use_pass) {
-        const int rc = launch_pass_form(e, mode, args, nrec, h_rec_cell);
+        const int rc = e->use_pass == 2 ? launch_resident_form(e, mode, args, nrec, h_rec_cell)
+                                        : launch_pass_form(e, mode, args, nrec, h_rec_cell);
         if (rc == PSDM_OK) {
             e->launches += 1;
             return PSDM_OK;
@@ -2433,7 +2538,8 @@ int psdm_engine_autotune(psdm_engine* e, const psdm_params* prm, int32_t ny, int
 
 int psdm_engine_set_pass_launch(psdm_engine* e, int32_t on) {
     TRY(check_engine(e));
-    e->use_pass = on != 0;
+    if (on < 0 || on > 2) return fail(PSDM_ERR_ARG, "pass launch form must be 0, 1 or 2 (got %d)", on);
+    e->use_pass = on;
     return PSDM_OK;
 }
 

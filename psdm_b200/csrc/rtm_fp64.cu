@@ -2,7 +2,7 @@
 // precision forms on the GPU (no counterpart in the reference, whose solvers
 // are FP32 throughout).
 //
-// The per-cell update is the one-step kernels' generic cell (rtm_step.cu,
+// The per-cell update is the one-step kernels' generic cell (rtm_device.cuh,
 // cell_generic) evaluated in double precision in the same order: the 2nd
 // and 1st derivative sums of src/solver_space_derivs_clean.f90 with the
 // reference's edge rule, the C-PML recursions of

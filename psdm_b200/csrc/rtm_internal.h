@@ -354,6 +354,63 @@ int pass_blocks_per_sm(int mode);
 // Launch one pass (modes 0, 1, 2) with `grid` co-resident blocks.
 int launch_pass(int mode, const PassParams& pp, int grid, void* stream);
 
+// ---- resident pass kernel (rtm_resident.cu) --------------------------------
+// One cooperative launch per pass with one block per region of the grid; a
+// block keeps its region's two wavefield levels in shared memory for the
+// whole pass and exchanges only the 3-cell ring with its neighbours through
+// the global wavefield buffers, waiting on their step counters.
+constexpr int kResWarps = 16;
+constexpr int kResThreads = 32 * kResWarps;
+constexpr int kResRows = 384;             // most rows of a region (a multiple of 4)
+constexpr int kResPitch = kResRows + 8;   // shared rows per column (4-row ring above and below)
+constexpr int kResMinSide = 8;            // fewest rows and columns of a region
+// Work item kinds of a warp (items[2k+1] = first quad or row
+// (region-relative) << 16 | first column (region-relative)):
+//   0  interior float4s: items[2k] = 0 | ncols << 4 | lanes << 8, lane l the
+//      float4 of quad first+l over ncols columns
+//   1  C-PML x-strip float4s (interior band rows): as 0, the x-strip update
+//   3  C-PML z-strip float4s (interior columns, rows away from the strip and
+//      grid edges): as 0, the z-strip update
+//   2  generic cells: items[2k] = 2 | groups << 4 | rows << 8 | span << 16,
+//      lane l row first + l % rows, columns [span*g/groups,
+//      span*(g+1)/groups) of the item with g = l / rows
+constexpr int kResFast = 0, kResXpml = 1, kResGen = 2, kResZpml = 3;
+struct ResRegion {
+    int zr0, nrows, x0, w;  // device rows [zr0, zr0+nrows) (multiples of 4) x columns [x0, x0+w)
+    int nbr0, nnbr;         // neighbour regions nbr[nbr0 ..)
+    int rec0, nrec;         // receivers rec[rec0 ..) (forward gather)
+};
+struct ResParams {
+    const StepArgs* base;   // [2], by step parity
+    const PassVar* var;     // [nsteps]
+    int nsteps;
+    int nreg;
+    int sw;                 // shared columns per level buffer (widest region + 6)
+    const ResRegion* reg;   // [nreg]
+    const int* nbr;
+    const int* rec;
+    const int* warp_first;  // [nreg * kResWarps + 1] offsets into items (pairs)
+    const int* items;       // [2 * nitems]
+    int* flags;             // [nreg] steps completed, zero at launch
+    int* abort;             // device word, zero at launch
+    int* err;               // the engine's error word
+};
+struct ResPlan {
+    std::vector<ResRegion> reg;
+    std::vector<int> nbr, rec, warp_first, items;
+    int sw = 0;
+};
+// Regions, neighbour lists, receiver lists and per-warp work items of the
+// resident form for the step plan `a` (plan_tiles) with at most max_regions
+// regions of at most max_sw - 6 columns.  False if the grid does not fit.
+bool plan_resident(const StepArgs& a, int max_regions, int max_sw, int nrec, const int* h_rec_cell, ResPlan* plan);
+// Widest shared-memory window (columns) of a resident block on this device,
+// and how many resident blocks fit per multiprocessor (0 on failure).
+int resident_max_sw();
+int resident_blocks_per_sm(int mode, int sw);
+// Launch one pass (modes 0 and 1) of the resident kernel, rp.nreg blocks.
+int launch_resident(int mode, const ResParams& rp, void* stream);
+
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
 int launch_wait_timeout_probe(int* err, void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.

@@ -81,106 +81,6 @@ constexpr int kPairFloats = kCleanFloats > kGenericFloats ? kCleanFloats : kGene
 // Largest |snapshot| of each sub-step seen by this block (float bits).
 __shared__ unsigned int s_pair_amax[2];
 
-// The packed FP32x2 interior update of the one-step interior tiles for one
-// float4 of rows: win = the 7 x-neighbour columns (centre win[3]), zm / zp =
-// the float4s above and below the centre, pmv = level n-1 of the float4,
-// c2v = its c2.  Tap sums and products are packed; every add that consumes
-// a fresh product is scalar, so no multiply-add is ever fused.
-__device__ __forceinline__ float4 clean_update(const float4 (&win)[7], const float4& zm, const float4& zp,
-                                               const float4& pmv, const float4& c2v, const float2 (&cc)[4]) {
-    const float4& pc = win[3];
-    const float2 z01 = make_float2(zm.y, zm.z), z12 = make_float2(zm.z, zm.w);
-    const float2 z23 = make_float2(zm.w, pc.x), z34 = lo2(pc);
-    const float2 z45 = make_float2(pc.y, pc.z), z56 = hi2(pc);
-    const float2 z67 = make_float2(pc.w, zp.x), z78 = lo2(zp);
-    const float2 z89 = make_float2(zp.y, zp.z);
-#define XA(k) lo2(win[3 + (k)])
-#define XB(k) hi2(win[3 + (k)])
-    const float2 d2xA = D2P(XA, cc);
-    const float2 d2xB = D2P(XB, cc);
-#undef XA
-#undef XB
-    const float2 zA[7] = {z01, z12, z23, z34, z45, z56, z67};
-    const float2 zB[7] = {z23, z34, z45, z56, z67, z78, z89};
-#define ZA(k) zA[3 + (k)]
-#define ZB(k) zB[3 + (k)]
-    const float2 d2yA = D2P(ZA, cc);
-    const float2 d2yB = D2P(ZB, cc);
-#undef ZA
-#undef ZB
-    // -p1 + 2p: 2p is exact, so a fused form would round identically
-    const float2 two = make_float2(2.f, 2.f);
-    const float2 baseA = __fadd2_rn(neg2(lo2(pmv)), __fmul2_rn(two, lo2(pc)));
-    const float2 baseB = __fadd2_rn(neg2(hi2(pmv)), __fmul2_rn(two, hi2(pc)));
-    const float2 oA = add_prod(baseA, __fmul2_rn(lo2(c2v), __fadd2_rn(d2xA, d2yA)));
-    const float2 oB = add_prod(baseB, __fmul2_rn(hi2(c2v), __fadd2_rn(d2xB, d2yB)));
-    return make_float4(oA.x, oA.y, oB.x, oB.y);
-}
-
-// Snapshot (forward) or imaging update (backward) of one float4 of interior
-// cells at offset fi of the pitched snapshot / image: out = the new level,
-// pmv = the level two steps back.  Fc / Ic / Cc / Frc: prefetched snapshot,
-// image, compensation and raw 16-bit snapshot values.
-template <int MODE>
-__device__ __forceinline__ void emit4(const StepArgs& a, const SubStep& s, int fi, const float4& out,
-                                      const float4& pmv, float4 Fc, const float4& Ic, const float4& Cc,
-                                      const uint2& Frc, float isc, float& amax_t) {
-    if (MODE == 0) {
-        const float hx = __fmul_rn(__fsub_rn(out.x, pmv.x), 0.5f);
-        const float hy = __fmul_rn(__fsub_rn(out.y, pmv.y), 0.5f);
-        const float hz = __fmul_rn(__fsub_rn(out.z, pmv.z), 0.5f);
-        const float hw = __fmul_rn(__fsub_rn(out.w, pmv.w), 0.5f);
-        bool rare = false;
-        float4 sv;
-        sv.x = div_dt_common(a, hx, rare);
-        sv.y = div_dt_common(a, hy, rare);
-        sv.z = div_dt_common(a, hz, rare);
-        sv.w = div_dt_common(a, hw, rare);
-        if (__any_sync(__activemask(), rare) && rare) {
-            sv.x = div_dt(a, hx);
-            sv.y = div_dt(a, hy);
-            sv.z = div_dt(a, hz);
-            sv.w = div_dt(a, hw);
-        }
-        *reinterpret_cast<float4*>(s.field + fi) = sv;
-        if (s.field_amax != nullptr)
-            amax_t = fmaxf(amax_t, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(sv.z), fabsf(sv.w))));
-    } else if (MODE == 1) {
-        if (s.field_w != 1.f) {
-            Fc.x = __fmul_rn(Fc.x, s.field_w); Fc.y = __fmul_rn(Fc.y, s.field_w);
-            Fc.z = __fmul_rn(Fc.z, s.field_w); Fc.w = __fmul_rn(Fc.w, s.field_w);
-        }
-        const float2 half = make_float2(0.5f, 0.5f);
-        const float2 oA = lo2(out), oB = hi2(out);
-        float2 iA = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oA, neg2(lo2(pmv)))), lo2(Fc));
-        float2 iB = __fmul2_rn(__fmul2_rn(half, __fadd2_rn(oB, neg2(hi2(pmv)))), hi2(Fc));
-        if (a.ss != 1.f) {
-            const float2 ss = make_float2(a.ss, a.ss);
-            iA = __fmul2_rn(iA, ss);
-            iB = __fmul2_rn(iB, ss);
-        }
-        const float2 rA = add_prod(lo2(Ic), iA), rB = add_prod(hi2(Ic), iB);
-        *reinterpret_cast<float4*>(a.image + fi) = make_float4(rA.x, rA.y, rB.x, rB.y);
-    } else {
-        const float4 F4 = unpack16x4(Frc, a.kind16, isc);
-        float Fv[4] = {F4.x, F4.y, F4.z, F4.w};
-        float Iv[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
-        float Cv[4] = {Cc.x, Cc.y, Cc.z, Cc.w};
-        const float ov[4] = {out.x, out.y, out.z, out.w};
-        const float pv[4] = {pmv.x, pmv.y, pmv.z, pmv.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            float F = Fv[e];
-            if (s.field_w != 1.f) F = __fmul_rn(F, s.field_w);
-            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(ov[e], pv[e])), F);
-            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
-            kahan(Iv[e], Cv[e], inc);
-        }
-        *reinterpret_cast<float4*>(a.image + fi) = make_float4(Iv[0], Iv[1], Iv[2], Iv[3]);
-        *reinterpret_cast<float4*>(a.comp + fi) = make_float4(Cv[0], Cv[1], Cv[2], Cv[3]);
-    }
-}
-
 // One phase of a clean interior tile (rows [z0, z0+nrows), a multiple of 4
 // starting on a float4 boundary; columns [x0, x0+ncols)).
 //   PH = 0: level n+1 on rows [z0-4, z0+nrows+4) x columns [x0-3,
@@ -388,7 +288,7 @@ __device__ __forceinline__ void pair_field(const PairArgs& P, int fi, float out,
 }
 
 // One cell of a generic tile at sub-step SUB: the one-step kernels' generic
-// cell update (rtm_step.cu, cell_generic) with its sources moved:
+// cell update (cell_generic, rtm_device.cuh) with its sources moved:
 //   SUB 0: stencil level n from S0, level n-1 / phi / chi at level n and the
 //     free-surface histories (levels n, n-1) from HBM; results to S1 and the
 //     phi / chi / history tiles, and on the tile to the level n+1 outputs;

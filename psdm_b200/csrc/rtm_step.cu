@@ -100,122 +100,6 @@ __device__ __forceinline__ void load_tile(const StepArgs& a, float* ps, int sz0,
     load_tile_from(a.p, a, ps, sz0, sx0, hq, wx, tid);
 }
 
-// Any cell of the grid: C-PML strips and corners, free-surface row,
-// injection, interior.  zd = device row (logical z = zd - zoff); the p tile
-// has SH rows per column and origin (sz0, sx0).
-template <int MODE, int SH>
-__device__ __forceinline__ void cell_generic(const StepArgs& a, const float* __restrict__ ps, int sz0, int sx0, int zd,
-                                             int x) {
-    const int dn = a.dn;
-    const int z = zd - a.zoff;
-    if (z < 0 || z >= a.nyt || x >= a.nxt) return;
-    // With a free surface the rows above it are never updated: p stays zero.
-    if (a.fs && z < dn) return;
-    const int kz = (z < dn) ? (dn - z) : (z >= dn + a.ny ? z - (dn + a.ny) + 1 : 0);
-    const int kx = (x < dn) ? (dn - x) : (x >= dn + a.nx ? x - (dn + a.nx) + 1 : 0);
-    const bool fsrow = a.fs && z == dn;
-    const int zl = zd - sz0, xl = x - sx0;
-    const int cxl = clampi(x, 3, a.nxt - 4) - sx0;
-    const int czl = clampi(z, 3, a.nyt - 4) + a.zoff - sz0;
-    const float* colc = ps + cxl * SH + zl;  // x-stencil centre
-    const float* colz = ps + xl * SH + czl;  // z-stencil centre
-#define AX(k) colc[(k) * SH]
-#define AZ(k) colz[(k)]
-    const float d2x = D2(AX, a.cf2);
-    const float d2y = D2(AZ, a.cf2);
-    const int g = x * a.ldz + zd;
-    const float pc = ps[xl * SH + zl];
-    const float pmo = a.pm[g];
-    const float c2v = __ldg(a.c2 + g);
-
-    float pp = pc, ppm = pmo;
-    if (fsrow && kx > 0 && !a.disk) { pp = a.side_p[x]; ppm = a.side_pm[x]; }
-    const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
-
-    float main_term, propz = 0.f;
-    if (kx > 0 || kz > 0) {
-        const int f = (kx > 0 && kz > 0) ? max(kx, kz) : (kx > 0 ? kx : kz);
-        const float A = __ldg(a.fA + f - 1), B = __ldg(a.fB + f - 1);
-        float propx = 0.f;
-        if (kx > 0) {
-            const float d1 = D1(AX, a.cf1);
-            const int sb = (x < dn) ? 0 : dn + a.nx;
-            const int ci = clampi(x - sb, 3, dn - 4) + sb;
-            const float* ph = a.phix_in + ci * a.ldz + zd;
-#define PX(k) ph[(k) * a.ldz]
-            const float dph = D1(PX, a.cf1);
-#undef PX
-            const float phn = __fadd_rn(__fmul_rn(A, a.phix_in[g]), __fmul_rn(B, d1));
-            const float chn = __fadd_rn(__fmul_rn(A, a.chix[g]), __fmul_rn(B, __fadd_rn(d2x, dph)));
-            a.phix_out[g] = phn;
-            a.chix[g] = chn;
-            propx = __fadd_rn(dph, chn);
-        }
-        if (kz > 0) {
-            const float d1 = D1(AZ, a.cf1);
-            const int sb = (z < dn) ? 0 : dn + a.ny;
-            const int cj = clampi(z - sb, 3, dn - 4) + sb + a.zoff;
-            const float* ph = a.phiz_in + x * a.ldz + cj;
-#define PZ(k) ph[(k)]
-            const float dph = D1(PZ, a.cf1);
-#undef PZ
-            const float phn = __fadd_rn(__fmul_rn(A, a.phiz_in[g]), __fmul_rn(B, d1));
-            const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
-            a.phiz_out[g] = phn;
-            a.chiz[g] = chn;
-            propz = __fadd_rn(dph, chn);
-        }
-        main_term = (kx > 0) ? propx : propz;
-    } else {
-        float src = 0.f;
-        if (a.row_slot != nullptr) {
-            const int rs = __ldg(a.row_slot + zd);
-            if (rs >= 0) {
-                const int j = __ldg(a.inj_cols + rs * a.nxt + x);
-                if (j >= 0) src = __ldg(a.inj_trace + (size_t)j * a.inj_ld + a.inj_t);
-            }
-        }
-        main_term = src;
-    }
-#undef AX
-#undef AZ
-    float p3 = __fadd_rn(base, __fmul_rn(c2v, __fadd_rn(__fadd_rn(d2x, d2y), main_term)));
-    if (kx > 0 && kz > 0) p3 = __fadd_rn(p3, __fmul_rn(c2v, propz));
-
-    float out = p3;
-    if (fsrow) {
-        if (kx > 0) {
-            if (!a.disk) { a.side_pm[x] = p3; out = 0.f; }
-        } else {
-            out = 0.f;
-        }
-    }
-    a.pm[g] = out;
-
-    if (kx == 0 && kz == 0 && a.field != nullptr) {
-        const int fi = (x - dn) * a.ldf + (z - dn);
-        if (MODE == 0) {
-            const float D = div_dt(a, __fmul_rn(__fsub_rn(out, pmo), 0.5f));
-            a.field[fi] = D;
-            if (a.field_amax != nullptr) amax_note(D);
-        } else {
-            float F = __ldg(a.field + fi);
-            if (a.field_w != 1.f) F = __fmul_rn(F, a.field_w);
-            float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
-            if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
-            a.image[fi] = __fadd_rn(a.image[fi], inc);
-        }
-    }
-    if (MODE == 2 && kx == 0 && kz == 0 && a.field16 != nullptr) {
-        const int fi = (x - dn) * a.ldf + (z - dn);
-        float F = load16x1(a.field16, fi, a.kind16, __ldg(a.field_iscale));
-        if (a.field_w != 1.f) F = __fmul_rn(F, a.field_w);
-        float inc = __fmul_rn(__fmul_rn(0.5f, __fsub_rn(out, pmo)), F);
-        if (a.ss != 1.f) inc = __fmul_rn(inc, a.ss);
-        kahan(a.image[fi], a.comp[fi], inc);
-    }
-}
-
 // Interior tile (rect type 0): rows [zd0, zd0+h) are interior rows without
 // injection and without the free-surface row, starting on a 16-byte
 // boundary; columns [x0, x0+w) are interior columns.  No stencil centre is
@@ -471,62 +355,11 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     const bool fsq = a.fs && z == dn;
     const float4* __restrict__ ps4 = reinterpret_cast<const float4*>(ps);
     const int qr = (zd - sz0) >> 2;
-    const float* c1 = a.cf1;
-    const float* c2 = a.cf2;
 #pragma unroll 1
     for (int c = 0; c < PXS; ++c) {
         const int x = x0 + wy * PXS + c;
         if (x >= xend) break;
-        const int kx = (x < dn) ? (dn - x) : (x - (dn + a.nx) + 1);
-        const int cx = clampi(x, 3, a.nxt - 4);
-        const int sb = (x < dn) ? 0 : dn + a.nx;
-        const int ci = clampi(x - sb, 3, dn - 4) + sb;
-        const float A = __ldg(a.fA + kx - 1), B = __ldg(a.fB + kx - 1);
-        const int g = x * a.ldz + zd;
-        float4 P[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) P[k] = ps4[(cx + k - 3 - sx0) * HQ + qr];
-        const float4 zc = ps4[(x - sx0) * HQ + qr];
-        const float4 zm = ps4[(x - sx0) * HQ + qr - 1];
-        const float4 zp = ps4[(x - sx0) * HQ + qr + 1];
-        float4 F[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k)
-            if (k != 3) F[k] = *reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd);
-        F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 phc = *reinterpret_cast<const float4*>(a.phix_in + g);
-        const float4 chc = *reinterpret_cast<const float4*>(a.chix + g);
-        const float4 pmv = *reinterpret_cast<const float4*>(a.pm + g);
-        const float4 c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
-        const float zv[10] = {zm.y, zm.z, zm.w, zc.x, zc.y, zc.z, zc.w, zp.x, zp.y, zp.z};
-        float o[4], phn[4], chn[4];
-#pragma unroll
-        for (int rr = 0; rr < 4; ++rr) {
-#define PXR(k) comp(P[3 + (k)], rr)
-#define FXR(k) comp(F[3 + (k)], rr)
-#define ZR(k) zv[3 + rr + (k)]
-            const float d2x = D2(PXR, c2);
-            const float d1x = D1(PXR, c1);
-            const float d2y = D2(ZR, c2);
-            const float dph = D1(FXR, c1);
-#undef PXR
-#undef FXR
-#undef ZR
-            phn[rr] = __fadd_rn(__fmul_rn(A, comp(phc, rr)), __fmul_rn(B, d1x));
-            chn[rr] = __fadd_rn(__fmul_rn(A, comp(chc, rr)), __fmul_rn(B, __fadd_rn(d2x, dph)));
-            const float prop = __fadd_rn(dph, chn[rr]);
-            float pp = comp(zc, rr), ppm = comp(pmv, rr);
-            if (rr == 0 && fsq && !a.disk) { pp = a.side_p[x]; ppm = a.side_pm[x]; }
-            const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
-            o[rr] = __fadd_rn(base, __fmul_rn(comp(c2v, rr), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
-        }
-        if (fsq && !a.disk) {  // free-surface row: private history keeps p3, the grid gets 0
-            a.side_pm[x] = o[0];
-            o[0] = 0.f;
-        }
-        *reinterpret_cast<float4*>(a.pm + g) = make_float4(o[0], o[1], o[2], o[3]);
-        *reinterpret_cast<float4*>(a.phix_out + g) = make_float4(phn[0], phn[1], phn[2], phn[3]);
-        *reinterpret_cast<float4*>(a.chix + g) = make_float4(chn[0], chn[1], chn[2], chn[3]);
+        xband_column<HQ>(a, ps4, nullptr, sx0, qr, zd, fsq, x);
     }
 }
 
@@ -781,44 +614,6 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
 }
 
 // ---- one launch per pass (dataflow form)
-
-__device__ __forceinline__ int ld_relaxed(const int* p) {
-    int v;
-    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-// Later bulk copies (async proxy) of this thread see what its generic-proxy
-// acquire made visible.
-__device__ __forceinline__ void fence_proxy_async_global() {
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Wait until *flag >= need: relaxed polls, then one acquire load.  Gives up
-// after ~1 s, or at once when another block has given up (abort, a device
-// word: polling the host-mapped error word would cost a PCIe round trip).
-__device__ bool wait_flag(const int* flag, int need, const int* abort) {
-    if (ld_relaxed(flag) < need) {
-        const uint64_t t0 = globaltimer_ns();
-        for (int it = 0;; ++it) {
-            if (ld_relaxed(flag) >= need) break;
-            if ((it & 15) == 15 && (ld_relaxed(abort) != 0 || globaltimer_ns() - t0 > 1000000000ull)) return false;
-        }
-    }
-    return ld_acquire(flag) >= need;  // the flag only grows
-}
 
 // All steps of one pass.  Block b owns tiles b, b + gridDim.x, ...; before
 // step i of a tile it waits until each neighbour tile has completed i steps

@@ -219,9 +219,10 @@ class Engine:
         """psdm_freq_filter_device: filters device traces (num, nt) in place (asynchronous)."""
         L.check(L.lib().psdm_freq_filter_device(self._h, d_traces, nt, dt, num, typef, f1, f2))
 
-    def set_pass_launch(self, on: bool):
-        """psdm_engine_set_pass_launch: one cooperative launch per pass (True) or one launch per step."""
-        L.check(L.lib().psdm_engine_set_pass_launch(self._h, int(bool(on))))
+    def set_pass_launch(self, on):
+        """psdm_engine_set_pass_launch: one launch per step (0 / False), one cooperative launch per pass
+        with tiles (1 / True) or with regions resident in shared memory (2)."""
+        L.check(L.lib().psdm_engine_set_pass_launch(self._h, int(on)))
 
     def set_steps_per_launch(self, steps: int):
         """psdm_engine_set_steps_per_launch: 2 (default) time steps per kernel launch, or 1."""

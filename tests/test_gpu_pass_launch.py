@@ -1,8 +1,11 @@
-"""One cooperative launch per pass (psdm_engine_set_pass_launch(1)) against
-one launch per time step: the same images, receiver traces and
+"""One cooperative launch per pass against one launch per time step, for
+both pass forms: tiles that re-read their inputs every step
+(psdm_engine_set_pass_launch(1)) and regions resident in shared memory
+(psdm_engine_set_pass_launch(2)).  The same images, receiver traces and
 mixed-precision images bit for bit, the images against the oracle, and the
 launch count showing which form ran.  The large case has more tiles than
-co-resident blocks, so blocks own several tiles."""
+co-resident blocks, so tile blocks own several tiles, and a config-2 window
+with its 480 receivers runs as resident regions."""
 import numpy as np
 import pytest
 
@@ -31,13 +34,13 @@ def _model(engine, c):
                              c["ny"], c["nx"], c["nx_w"], c["vp_w"], c["added_space"], c["nt"])
 
 
-def _both(engine, fn):
-    """fn() with one launch per pass, then with one launch per time step, and
-    the engine's launch counts of each; the engine is left in its default
-    form (one step per launch)."""
+def _both(engine, fn, form=1):
+    """fn() with one launch per pass (form 1 or 2), then with one launch per
+    time step, and the engine's launch counts of each; the engine is left in
+    its default form (one step per launch)."""
     out = []
     try:
-        for on in (True, False):
+        for on in (form, 0):
             engine.set_pass_launch(on)
             engine.set_steps_per_launch(1)
             engine.reset_stats()
@@ -65,10 +68,11 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("ci", range(len(CASES)))
-def test_pass_launch_image_exact(engine, oracle, ci):
+def test_pass_launch_image_exact(engine, oracle, ci, form):
     c = make_case(**CASES[ci])
-    (img_p, n_p), (img_s, n_s) = _both(engine, lambda: _rtm(engine, c))
+    (img_p, n_p), (img_s, n_s) = _both(engine, lambda: _rtm(engine, c), form)
     _same(img_p, img_s, "PSDM_w pass vs step launches")
     assert n_p < 20 and n_s >= 2 * (c["nt"] - 1), (n_p, n_s)
     want = oracle.rtm_shot(dPML=c["dPML"], fs=c["fs"], nxSou=c["nxSou"], nySou=c["nySou"], nxRec=c["nxRec"],
@@ -80,10 +84,11 @@ def test_pass_launch_image_exact(engine, oracle, ci):
     _same(img_p, want, "PSDM_w pass launch vs oracle")
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("ci", [0, 1, 3])
-def test_pass_launch_receivers_exact(engine, ci):
+def test_pass_launch_receivers_exact(engine, ci, form):
     c = make_case(**CASES[ci])
-    (rec_p, n_p), (rec_s, _) = _both(engine, lambda: _model(engine, c))
+    (rec_p, n_p), (rec_s, _) = _both(engine, lambda: _model(engine, c), form)
     _same(rec_p, rec_s, "Rec_point pass vs step launches")
     assert n_p < 10
 
@@ -93,6 +98,29 @@ def test_pass_launch_mixed_backward_exact(engine):
     (img_p, n_p), (img_s, n_s) = _both(engine, lambda: _rtm(engine, c, FP16, 4))
     _same(img_p, img_s, "mixed PSDM_w pass vs step launches")
     assert n_p < n_s
+
+
+def test_resident_mixed_falls_back_to_steps(engine):
+    """The resident form leaves the mixed-precision passes to one launch per
+    step: same image, more launches than a resident shot."""
+    c = make_case(**CASES[1])
+    (img_p, n_p), (img_s, n_s) = _both(engine, lambda: _rtm(engine, c, FP16, 4), 2)
+    _same(img_p, img_s, "mixed PSDM_w resident vs step launches")
+
+
+def test_resident_config2_window(engine):
+    """The config-2 window (1200 x 1136 cells, CPML 50, free surface, 480
+    receivers on a 12.5 m spread) as resident regions: image and receiver
+    traces equal one launch per step."""
+    c = make_case(ny=1200, nx_model=1600, dd=6.25, dt=5e-4, nt=80, dPML=50, fs=1, nrec=480, rec_step=2, sou_x=1100,
+                  sou_z=2, rec_z=2, added_space=540.0, seed=7)
+    assert c["nx_w"] == 1136
+    (img_p, n_p), (img_s, _) = _both(engine, lambda: _rtm(engine, c), 2)
+    _same(img_p, img_s, "PSDM_w resident vs step launches (config-2 window)")
+    assert n_p < 10
+    (rec_p, n_p), (rec_s, _) = _both(engine, lambda: _model(engine, c), 2)
+    _same(rec_p, rec_s, "Rec_point resident vs step launches (config-2 window)")
+    assert n_p < 10
 
 
 def test_pass_launch_many_tiles_per_block(engine):
