@@ -247,6 +247,7 @@ def run_reference(args):
 # FP32 shots; spl = time steps per kernel launch.
 FORMS = [
     dict(name="fp32_two_steps", precision=0, ks=1, slots=0, spl=2),
+    dict(name="fp32_resident", precision=0, ks=1, slots=0, pass_form=2),
     dict(name="fp16_ks4", precision=1, ks=4, slots=0),
     dict(name="batch_fp16_ks4", precision=1, ks=4, slots=8),
     dict(name="batch_bf16_ks4", precision=2, ks=4, slots=8),
@@ -343,6 +344,7 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         engine.set_checkpointing(ckpt)
         engine.set_reconstruction(f.get("recon", False))
         engine.set_steps_per_launch(f.get("spl", 1))
+        engine.set_pass_launch(f.get("pass_form", 0))
         sel = [(items[i % len(items)], outs[i % len(outs)]) for i in range(n)]
 
         def run(k):
@@ -368,6 +370,7 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
         engine.set_checkpointing(0)
         engine.set_reconstruction(False)
         engine.set_steps_per_launch(1)
+        engine.set_pass_launch(0)
         v = n / (e0.elapsed_time(e1) / 1e3)
         out[name] = {"shots_per_s": v, "vs_plain": v / ref_value, "shots": n,
                      "slots": engine.batch_slots() if slots else 1, "precision": ["f32", "fp16", "bf16"][precision],
@@ -378,6 +381,8 @@ def time_forms(engine, torch, dev, stream, d_src, items, names, ref_value):
             out[name]["steps_per_launch"] = f["spl"]
         if f.get("recon"):
             out[name]["source_wavefield"] = "reconstructed from a saved 3-cell band"
+        if f.get("pass_form"):
+            out[name]["launch"] = "one cooperative launch per pass, regions resident in shared memory"
     return out
 
 

@@ -446,21 +446,43 @@ __device__ __forceinline__ void emit4(const StepArgs& a, const SubStep& s, int f
 }
 
 // One column x of a C-PML x-strip (kz = 0) for the float4 of rows zd..zd+3
-// (a multiple of 4): p at level n from the shared tile ps4 (HQP float4 rows
-// per column, origin column sx0, float4 row qr of zd), phi, chi, c2 and
-// (without RES) level n-1 from global memory.  RES: level n-1 is read from,
-// and the new level also stored to, the shared tile pps4.
-template <int HQP, bool RES = false>
-__device__ __forceinline__ void xband_column(const StepArgs& a, const float4* __restrict__ ps4, float4* pps4,
-                                             int sx0, int qr, int zd, bool fsq, int x) {
+// (a multiple of 4), split into its global loads (xband_load: phi_x around
+// the strip-local stencil centre, phi_x, chi_x and c2 of the cells, and level
+// n-1 unless it comes from shared memory) and its update (xband_compute), so
+// that callers can load the next column while they update this one.  p at
+// level n comes from the shared tile ps4 (HQP float4 rows per column, origin
+// column sx0, float4 row qr of zd).  RES: level n-1 is read from, and the new
+// level also stored to, the shared tile pps4.
+struct XbandIn {
+    float4 F[7];  // phi_x stencil around the strip-local centre (F[3] unused)
+    float4 phc, chc, c2v, pmv;
+    float A, B;
+};
+
+__device__ __forceinline__ void xband_load(const StepArgs& a, int zd, int x, bool load_pm, XbandIn& in) {
     const int dn = a.dn;
-    const float* c1 = a.cf1;
-    const float* c2 = a.cf2;
     const int kx = (x < dn) ? (dn - x) : (x - (dn + a.nx) + 1);
-    const int cx = clampi(x, 3, a.nxt - 4);
     const int sb = (x < dn) ? 0 : dn + a.nx;
     const int ci = clampi(x - sb, 3, dn - 4) + sb;
-    const float A = __ldg(a.fA + kx - 1), B = __ldg(a.fB + kx - 1);
+    in.A = __ldg(a.fA + kx - 1);
+    in.B = __ldg(a.fB + kx - 1);
+    const int g = x * a.ldz + zd;
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        if (k != 3) in.F[k] = *reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd);
+    in.F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+    in.phc = *reinterpret_cast<const float4*>(a.phix_in + g);
+    in.chc = *reinterpret_cast<const float4*>(a.chix + g);
+    in.c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
+    if (load_pm) in.pmv = *reinterpret_cast<const float4*>(a.pm + g);
+}
+
+template <int HQP, bool RES = false>
+__device__ __forceinline__ void xband_compute(const StepArgs& a, const float4* __restrict__ ps4, float4* pps4, int sx0,
+                                              int qr, int zd, bool fsq, int x, const XbandIn& in) {
+    const float* c1 = a.cf1;
+    const float* c2 = a.cf2;
+    const int cx = clampi(x, 3, a.nxt - 4);
     const int g = x * a.ldz + zd;
     float4 P[7];
 #pragma unroll
@@ -468,21 +490,13 @@ __device__ __forceinline__ void xband_column(const StepArgs& a, const float4* __
     const float4 zc = ps4[(x - sx0) * HQP + qr];
     const float4 zm = ps4[(x - sx0) * HQP + qr - 1];
     const float4 zp = ps4[(x - sx0) * HQP + qr + 1];
-    float4 F[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k)
-        if (k != 3) F[k] = *reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd);
-    F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 phc = *reinterpret_cast<const float4*>(a.phix_in + g);
-    const float4 chc = *reinterpret_cast<const float4*>(a.chix + g);
-    const float4 pmv = RES ? pps4[(x - sx0) * HQP + qr] : *reinterpret_cast<const float4*>(a.pm + g);
-    const float4 c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
+    const float4 pmv = RES ? pps4[(x - sx0) * HQP + qr] : in.pmv;
     const float zv[10] = {zm.y, zm.z, zm.w, zc.x, zc.y, zc.z, zc.w, zp.x, zp.y, zp.z};
     float o[4], phn[4], chn[4];
 #pragma unroll
     for (int rr = 0; rr < 4; ++rr) {
 #define PXR(k) comp(P[3 + (k)], rr)
-#define FXR(k) comp(F[3 + (k)], rr)
+#define FXR(k) comp(in.F[3 + (k)], rr)
 #define ZR(k) zv[3 + rr + (k)]
         const float d2x = D2(PXR, c2);
         const float d1x = D1(PXR, c1);
@@ -491,20 +505,21 @@ __device__ __forceinline__ void xband_column(const StepArgs& a, const float4* __
 #undef PXR
 #undef FXR
 #undef ZR
-        phn[rr] = __fadd_rn(__fmul_rn(A, comp(phc, rr)), __fmul_rn(B, d1x));
-        chn[rr] = __fadd_rn(__fmul_rn(A, comp(chc, rr)), __fmul_rn(B, __fadd_rn(d2x, dph)));
+        phn[rr] = __fadd_rn(__fmul_rn(in.A, comp(in.phc, rr)), __fmul_rn(in.B, d1x));
+        chn[rr] = __fadd_rn(__fmul_rn(in.A, comp(in.chc, rr)), __fmul_rn(in.B, __fadd_rn(d2x, dph)));
         const float prop = __fadd_rn(dph, chn[rr]);
         float pp = comp(zc, rr), ppm = comp(pmv, rr);
         if (rr == 0 && fsq && !a.disk) { pp = a.side_p[x]; ppm = a.side_pm[x]; }
         const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
-        o[rr] = __fadd_rn(base, __fmul_rn(comp(c2v, rr), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+        o[rr] = __fadd_rn(base, __fmul_rn(comp(in.c2v, rr), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
     }
     if (fsq && !a.disk) {  // free-surface row: private history keeps p3, the grid gets 0
         a.side_pm[x] = o[0];
         o[0] = 0.f;
     }
-    *reinterpret_cast<float4*>(a.pm + g) = make_float4(o[0], o[1], o[2], o[3]);
-    if (RES) pps4[(x - sx0) * HQP + qr] = make_float4(o[0], o[1], o[2], o[3]);
+    const float4 out = make_float4(o[0], o[1], o[2], o[3]);
+    *reinterpret_cast<float4*>(a.pm + g) = out;
+    if (RES) pps4[(x - sx0) * HQP + qr] = out;
     *reinterpret_cast<float4*>(a.phix_out + g) = make_float4(phn[0], phn[1], phn[2], phn[3]);
     *reinterpret_cast<float4*>(a.chix + g) = make_float4(chn[0], chn[1], chn[2], chn[3]);
 }

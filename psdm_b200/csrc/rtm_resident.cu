@@ -373,82 +373,16 @@ __device__ __noinline__ void res_zpml_item(const StepArgs& a, const float4* ps4,
 }
 
 // An x-strip item's lane: the float4 of rows zd..zd+3 (interior band rows,
-// x in a C-PML x-strip) over columns x0..x0+ncol-1, with xband_column's
-// arithmetic in its order and the next column's global loads (phi_x
-// stencil, phi_x, chi_x, c2) in flight while the current column updates.
-struct XIn {
-    float4 F[7];  // phi_x stencil around the strip-local centre (F[3] unused)
-    float4 phc, chc, c2v;
-    float A, B;
-};
-
-__device__ __forceinline__ void res_xpml_load(const StepArgs& a, int zd, int x, XIn& in) {
-    const int dn = a.dn;
-    const int kx = (x < dn) ? (dn - x) : (x - (dn + a.nx) + 1);
-    const int sb = (x < dn) ? 0 : dn + a.nx;
-    const int ci = clampi(x - sb, 3, dn - 4) + sb;
-    in.A = __ldg(a.fA + kx - 1);
-    in.B = __ldg(a.fB + kx - 1);
-    const int g = x * a.ldz + zd;
-#pragma unroll
-    for (int k = 0; k < 7; ++k)
-        if (k != 3) in.F[k] = *reinterpret_cast<const float4*>(a.phix_in + (ci + k - 3) * a.ldz + zd);
-    in.F[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-    in.phc = *reinterpret_cast<const float4*>(a.phix_in + g);
-    in.chc = *reinterpret_cast<const float4*>(a.chix + g);
-    in.c2v = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
-}
-
+// x in a C-PML x-strip) over columns x0..x0+ncol-1, the next column's global
+// loads in flight while the current column updates.
 __device__ __noinline__ void res_xpml_item(const StepArgs& a, const float4* ps4, float4* pp4, int sx0, int qr, int zd,
                                            bool fsq, int x0, int ncol) {
-    const float* c1 = a.cf1;
-    const float* c2 = a.cf2;
-    XIn cur, nxt;
-    res_xpml_load(a, zd, x0, cur);
+    XbandIn cur, nxt;
+    xband_load(a, zd, x0, false, cur);
 #pragma unroll 1
     for (int c = 0; c < ncol; ++c) {
-        const int x = x0 + c;
-        if (c + 1 < ncol) res_xpml_load(a, zd, x + 1, nxt);
-        const int cx = clampi(x, 3, a.nxt - 4);
-        const int g = x * a.ldz + zd;
-        float4 P[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) P[k] = ps4[(cx + k - 3 - sx0) * RHQ + qr];
-        const float4 zc = ps4[(x - sx0) * RHQ + qr];
-        const float4 zm = ps4[(x - sx0) * RHQ + qr - 1];
-        const float4 zp = ps4[(x - sx0) * RHQ + qr + 1];
-        const float4 pmv = pp4[(x - sx0) * RHQ + qr];
-        const float zv[10] = {zm.y, zm.z, zm.w, zc.x, zc.y, zc.z, zc.w, zp.x, zp.y, zp.z};
-        float o[4], phn[4], chn[4];
-#pragma unroll
-        for (int rr = 0; rr < 4; ++rr) {
-#define PXR(k) comp(P[3 + (k)], rr)
-#define FXR(k) comp(cur.F[3 + (k)], rr)
-#define ZR(k) zv[3 + rr + (k)]
-            const float d2x = D2(PXR, c2);
-            const float d1x = D1(PXR, c1);
-            const float d2y = D2(ZR, c2);
-            const float dph = D1(FXR, c1);
-#undef PXR
-#undef FXR
-#undef ZR
-            phn[rr] = __fadd_rn(__fmul_rn(cur.A, comp(cur.phc, rr)), __fmul_rn(cur.B, d1x));
-            chn[rr] = __fadd_rn(__fmul_rn(cur.A, comp(cur.chc, rr)), __fmul_rn(cur.B, __fadd_rn(d2x, dph)));
-            const float prop = __fadd_rn(dph, chn[rr]);
-            float pp = comp(zc, rr), ppm = comp(pmv, rr);
-            if (rr == 0 && fsq && !a.disk) { pp = a.side_p[x]; ppm = a.side_pm[x]; }
-            const float base = __fadd_rn(-ppm, __fmul_rn(2.f, pp));
-            o[rr] = __fadd_rn(base, __fmul_rn(comp(cur.c2v, rr), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
-        }
-        if (fsq && !a.disk) {  // free-surface row: private history keeps p3, the grid gets 0
-            a.side_pm[x] = o[0];
-            o[0] = 0.f;
-        }
-        const float4 out = make_float4(o[0], o[1], o[2], o[3]);
-        *reinterpret_cast<float4*>(a.pm + g) = out;
-        pp4[(x - sx0) * RHQ + qr] = out;
-        *reinterpret_cast<float4*>(a.phix_out + g) = make_float4(phn[0], phn[1], phn[2], phn[3]);
-        *reinterpret_cast<float4*>(a.chix + g) = make_float4(chn[0], chn[1], chn[2], chn[3]);
+        if (c + 1 < ncol) xband_load(a, zd, x0 + c + 1, false, nxt);
+        xband_compute<RHQ, true>(a, ps4, pp4, sx0, qr, zd, fsq, x0 + c, cur);
         cur = nxt;
     }
 }

@@ -359,14 +359,20 @@ __device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, 
     for (int c = 0; c < PXS; ++c) {
         const int x = x0 + wy * PXS + c;
         if (x >= xend) break;
-        xband_column<HQ>(a, ps4, nullptr, sx0, qr, zd, fsq, x);
+        XbandIn in;
+        xband_load(a, zd, x, true, in);
+        xband_compute<HQ>(a, ps4, nullptr, sx0, qr, zd, fsq, x, in);
     }
 }
 
 // C-PML z-strip over interior columns (rect type 2): kx = 0.  Rows with
 // kz > 0 run a specialised update; interior rows of a partial float4 at the
-// bottom of the band fall back to the generic cell.
-template <int MODE>
+// bottom of the band fall back to the generic cell.  PF: each thread loads
+// the next column's global inputs while it updates the current one (the
+// one-shot FP32 step kernels, where these tiles end last; the mixed-precision,
+// batched and pass kernels keep the plain loop, whose lower register demand
+// suits them).
+template <int MODE, bool PF = false>
 __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r, int t) {
     const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
@@ -399,10 +405,58 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     const int cj = clampi(z - sb, 3, dn - 4) + sb + a.zoff;
     const float* c1 = a.cf1;
     const float* c2 = a.cf2;
+    if constexpr (!PF) {
+    #pragma unroll 1
+        for (int c = 0; c < ZXS; ++c) {
+            const int x = x0 + wy * ZXS + c;
+            if (x >= xend) break;
+            const int xl = x - sx0;
+            const float* colc = ps + xl * PHZ + zl;
+            const float* colz = ps + xl * PHZ + czl;
+    #define AX(k) colc[(k) * PHZ]
+    #define AZ(k) colz[(k)]
+            const float d2x = D2(AX, c2);
+            const float d2y = D2(AZ, c2);
+            const float d1 = D1(AZ, c1);
+    #undef AX
+            const int g = x * a.ldz + zd;
+            const float* phs = a.phiz_in + x * a.ldz;
+    #define PZ(k) phs[cj + (k)]
+            const float dph = D1(PZ, c1);
+    #undef PZ
+    #undef AZ
+            const float phn = __fadd_rn(__fmul_rn(A, phs[zd]), __fmul_rn(B, d1));
+            const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
+            a.phiz_out[g] = phn;
+            a.chiz[g] = chn;
+            const float prop = __fadd_rn(dph, chn);
+            const float base = __fadd_rn(-a.pm[g], __fmul_rn(2.f, colc[0]));
+            a.pm[g] = __fadd_rn(base, __fmul_rn(__ldg(a.c2 + g), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+        }
+        return;
+    }
+    // global inputs of one column: phi_z around the strip-local centre cj,
+    // phi_z, chi_z, level n-1 and c2 of the cell; the next column's are in
+    // flight during this column's update
+    struct ZIn { float f[7], ph, ch, pm, c2; };
+    auto zload = [&](int x, ZIn& v) {
+        const float* phs = a.phiz_in + x * a.ldz;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            if (k != 3) v.f[k] = phs[cj + k - 3];
+        const int g = x * a.ldz + zd;
+        v.ph = phs[zd];
+        v.ch = a.chiz[g];
+        v.pm = a.pm[g];
+        v.c2 = __ldg(a.c2 + g);
+    };
+    const int xb = x0 + wy * ZXS, xe = min(xb + ZXS, xend);
+    if (xb >= xe) return;
+    ZIn cur, nxt;
+    zload(xb, cur);
 #pragma unroll 1
-    for (int c = 0; c < ZXS; ++c) {
-        const int x = x0 + wy * ZXS + c;
-        if (x >= xend) break;
+    for (int x = xb; x < xe; ++x) {
+        if (x + 1 < xe) zload(x + 1, nxt);
         const int xl = x - sx0;
         const float* colc = ps + xl * PHZ + zl;
         const float* colz = ps + xl * PHZ + czl;
@@ -412,19 +466,19 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
         const float d2y = D2(AZ, c2);
         const float d1 = D1(AZ, c1);
 #undef AX
+#undef AZ
         const int g = x * a.ldz + zd;
-        const float* phs = a.phiz_in + x * a.ldz;
-#define PZ(k) phs[cj + (k)]
+#define PZ(k) cur.f[3 + (k)]
         const float dph = D1(PZ, c1);
 #undef PZ
-#undef AZ
-        const float phn = __fadd_rn(__fmul_rn(A, phs[zd]), __fmul_rn(B, d1));
-        const float chn = __fadd_rn(__fmul_rn(A, a.chiz[g]), __fmul_rn(B, __fadd_rn(d2y, dph)));
+        const float phn = __fadd_rn(__fmul_rn(A, cur.ph), __fmul_rn(B, d1));
+        const float chn = __fadd_rn(__fmul_rn(A, cur.ch), __fmul_rn(B, __fadd_rn(d2y, dph)));
         a.phiz_out[g] = phn;
         a.chiz[g] = chn;
         const float prop = __fadd_rn(dph, chn);
-        const float base = __fadd_rn(-a.pm[g], __fmul_rn(2.f, colc[0]));
-        a.pm[g] = __fadd_rn(base, __fmul_rn(__ldg(a.c2 + g), __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+        const float base = __fadd_rn(-cur.pm, __fmul_rn(2.f, colc[0]));
+        a.pm[g] = __fadd_rn(base, __fmul_rn(cur.c2, __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+        cur = nxt;
     }
 }
 
@@ -497,7 +551,7 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
                 if (!interior_tile<MODE, XS_ONE>(a, sm, &bar, phase, r, t)) return;
                 break;
             case 1: xband_tile<MODE>(a, sm, r, t); break;
-            case 2: zstrip_tile<MODE>(a, sm, r, t); break;
+            case 2: zstrip_tile<MODE, MODE != 2>(a, sm, r, t); break;
             case 4: rowband_tile<MODE>(a, sm, r, t); break;
             default: generic_tile<MODE>(a, sm, r, t); break;
         }
