@@ -82,6 +82,7 @@ constexpr int ZXS = 8;
 constexpr int ZTX = NWARP * ZXS;
 constexpr int ZWX = ZTX + 6;
 constexpr int RTX = 64;
+constexpr int kRing = 3;  // columns of p1 / c2 in flight per thread (RG)
 
 // Stage rows [sz0, sz0+4*hq) x columns [sx0, sx0+wx) of p in shared memory
 // (zero outside the array).  sz0 is a multiple of 4.
@@ -114,7 +115,7 @@ __device__ __forceinline__ void load_tile(const StepArgs& a, float* ps, int sz0,
 // ST: p1 and c2 of the tile are copied into shared memory with p (batched
 // launches, whose operands come from HBM rather than L2: every load of the
 // tile is in flight at once), instead of being read one column ahead.
-template <int MODE, int XS, bool ST = false>
+template <int MODE, int XS, bool ST = false, bool RG = false>
 __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int r,
                                               int t) {
     constexpr int TX = tile_cols(XS);
@@ -173,7 +174,21 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     float* __restrict__ pmp = a.pm;
     int g = (x0 + c0) * a.ldz + zd;
     float4 pmN = make_float4(0.f, 0.f, 0.f, 0.f), c2N = pmN;
-    if (active && !ST) {
+    // RG: this thread's p1 and c2 of the next kRing columns are copied into a
+    // ring of shared slots by cp.async, one commit group per column (groups
+    // past the last column are empty), so that kRing columns of HBM loads
+    // are in flight without holding registers.
+    float4* ring = reinterpret_cast<float4*>(sm + tile_smem_cols(XS) * HZ) + (threadIdx.y * 32 + lane);
+    if (RG && active) {
+#pragma unroll
+        for (int k = 0; k < kRing; ++k) {
+            if (c0 + k < ncols && k < XS) {
+                cp_async16(ring + (2 * k) * NT, pmp + g + k * a.ldz);
+                cp_async16(ring + (2 * k + 1) * NT, a.c2 + g + k * a.ldz);
+            }
+            cp_async_commit();
+        }
+    } else if (active && !ST) {
         pmN = *reinterpret_cast<const float4*>(pmp + g);
         c2N = __ldg(reinterpret_cast<const float4*>(a.c2 + g));
     }
@@ -181,6 +196,7 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(a.err, 1);
+        if (RG) cp_async_wait_all();
         return false;
     }
     if (!active) return true;
@@ -202,7 +218,17 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         const float4 zm = ps4[(col + 3) * HQ + qr - 1];
         const float4 zp = ps4[(col + 3) * HQ + qr + 1];
         float4 pmv = pmN, c2v = c2N;
-        if (ST) {
+        if (RG) {
+            cp_async_wait_group<kRing - 1>();  // column c's copies have landed
+            const int sl = c % kRing;
+            pmv = ring[(2 * sl) * NT];
+            c2v = ring[(2 * sl + 1) * NT];
+            if (c + kRing < ncol) {
+                cp_async16(ring + (2 * sl) * NT, pmp + g + kRing * a.ldz);
+                cp_async16(ring + (2 * sl + 1) * NT, a.c2 + g + kRing * a.ldz);
+            }
+            cp_async_commit();
+        } else if (ST) {
             pmv = *reinterpret_cast<const float4*>(pms + col * TZ + q);
             c2v = *reinterpret_cast<const float4*>(c2s + col * TZ + q);
         } else if (c + 1 < ncol) {
@@ -310,6 +336,7 @@ __device__ __forceinline__ bool interior_tile(const StepArgs& a, float* sm, uint
         g += a.ldz;
         fi += a.ldf;
     }
+    if (RG) cp_async_wait_all();  // the ring is reused by the next tile
     if (MODE == 0 && a.field_amax != nullptr && a.field != nullptr) amax_note(amax_t);
     return true;
 }
@@ -522,10 +549,23 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
         mbar_init(&bar, 1);
         s_blk_amax = 0u;
     }
+    // Receivers of the previous step (p is that step's p3, read-only during
+    // this step): spread over the blocks, a receiver per thread, loaded before
+    // the tiles and stored after them so that the load's latency overlaps the
+    // tiles' work.
+    int rec_i = -1;
+    float rec_v = 0.f;
     if (MODE == 0 && a.rec_t >= 0) {
-        // Receivers of the previous step: p is that step's p3.
-        for (int i = blockIdx.x * NT + tid; i < a.nrec; i += gridDim.x * NT)
-            a.rec_out[(size_t)i * a.rec_ld + a.rec_t] = a.p[a.rec_cell[i]];
+        if (a.nrec <= (int)gridDim.x * NT) {
+            const int i = blockIdx.x + (int)gridDim.x * tid;
+            if (i < a.nrec) {
+                rec_i = i;
+                rec_v = a.p[a.rec_cell[i]];
+            }
+        } else {
+            for (int i = blockIdx.x * NT + tid; i < a.nrec; i += gridDim.x * NT)
+                a.rec_out[(size_t)i * a.rec_ld + a.rec_t] = a.p[a.rec_cell[i]];
+        }
     }
     if (MODE == 0 && a.q_src != nullptr) quantize_part(a.q_src, a.q_amax, a.q_dst, a.q_iscale, a.q_n, a.kind16, tid);
     // Persistent blocks take tiles in order (heaviest rect types first) from
@@ -541,6 +581,7 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
         if (b >= total) {
             if (MODE == 0 && tid == 0 && a.field_amax != nullptr && s_blk_amax != 0u)
                 atomicMax(a.field_amax, s_blk_amax);
+            if (MODE == 0 && rec_i >= 0) a.rec_out[(size_t)rec_i * a.rec_ld + a.rec_t] = rec_v;
             return;
         }
         int r = 0;
@@ -569,17 +610,29 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
 // and on the B200 8 FP16 shots in flight ran at 5.73 against 6.32 shots/s
 // without it (config 4: 3.62 against 4.66).
 constexpr bool kBatchStage = PSDM_BATCH_STAGE != 0;
+// Batched launches whose slots are all in one pass, whose interior operands
+// come from HBM, prefetch p1 and c2 kRing columns ahead through a shared ring
+// (interior_tile's RG): 8 FP16 shots in flight ran at 6.75 against 6.33
+// shots/s without it on the B200.  The instance for slots in different
+// passes keeps one column ahead in registers (with the ring config 4 ran at
+// 3.3-3.8 against 4.2-4.5 shots/s).
+#ifndef PSDM_BATCH_RING
+#define PSDM_BATCH_RING 1
+#endif
+constexpr bool kBatchRing = PSDM_BATCH_RING != 0 && !kBatchStage;
 constexpr int batch_smem_floats() {
-    return smem_floats<XS_MANY>() + (kBatchStage ? 2 * TZ * tile_cols(XS_MANY) : 0);
+    return smem_floats<XS_MANY>() + (kBatchStage ? 2 * TZ * tile_cols(XS_MANY) : 0) +
+           (kBatchRing ? 4 * 2 * kRing * NT : 0);
 }
 
-template <int MODE, int XS = XS_MANY, bool ST = (XS == XS_MANY && kBatchStage)>
+template <int MODE, int XS = XS_MANY, bool ST = (XS == XS_MANY && kBatchStage),
+          bool RG = (XS == XS_MANY && kBatchRing)>
 __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t* bar, uint32_t& phase, int b) {
     int r = 0;
     while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
     const int t = b - a.r_first[r];
     switch (a.r_type[r]) {
-        case 0: return interior_tile<MODE, XS, ST>(a, sm, bar, phase, r, t);
+        case 0: return interior_tile<MODE, XS, ST, RG>(a, sm, bar, phase, r, t);
         case 1: xband_tile<MODE>(a, sm, r, t); return true;
         case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
         case 4: rowband_tile<MODE>(a, sm, r, t); return true;
@@ -658,9 +711,11 @@ __global__ void __launch_bounds__(NT, 5) batch_step_kernel(const BatchParams bp)
         if (FIXED >= 0) {
             ok = run_tile<(FIXED >= 0 ? FIXED : 0)>(sa, sm, &bar, phase, lb);
         } else {
+            // slots in different passes: no p1/c2 ring (measured slower in this instance)
             const int md = bp.mode[s];
-            ok = md == 0 ? run_tile<0>(sa, sm, &bar, phase, lb)
-                         : (md == 1 ? run_tile<1>(sa, sm, &bar, phase, lb) : run_tile<2>(sa, sm, &bar, phase, lb));
+            ok = md == 0 ? run_tile<0, XS_MANY, kBatchStage, false>(sa, sm, &bar, phase, lb)
+                         : (md == 1 ? run_tile<1, XS_MANY, kBatchStage, false>(sa, sm, &bar, phase, lb)
+                                    : run_tile<2, XS_MANY, kBatchStage, false>(sa, sm, &bar, phase, lb));
         }
         if (!ok) return;
         __syncthreads();  // shared tile, tile_id and (next switch) sa are reused
