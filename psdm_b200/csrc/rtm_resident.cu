@@ -369,7 +369,6 @@ __device__ __noinline__ void res_zpml_item(const StepArgs& a, const float4* ps4,
         c2v = nc2;
         g += a.ldz;
     }
-    (void)dn;
 }
 
 // An x-strip item's lane: the float4 of rows zd..zd+3 (interior band rows,
@@ -493,7 +492,7 @@ __global__ void __launch_bounds__(kResThreads, 1) res_kernel(const ResParams rp)
     if (tid == 0) cp_async_wait_all();
 }
 
-template <int MODE>
+// Dynamic shared memory of a resident block: two level buffers of sw columns.
 int res_smem_bytes(int sw) {
     return 2 * RSH * sw * (int)sizeof(float);
 }
@@ -801,7 +800,7 @@ int resident_max_sw() {
 
 template <int MODE>
 int res_blocks_t(int sw) {
-    const int bytes = res_smem_bytes<MODE>(sw);
+    const int bytes = res_smem_bytes(sw);
     if (cudaFuncSetAttribute(res_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
         return 0;
     int n = 0;
@@ -819,7 +818,7 @@ int resident_blocks_per_sm(int mode, int sw) {
 
 template <int MODE>
 int launch_res_t(const ResParams& rp, cudaStream_t stream) {
-    const int bytes = res_smem_bytes<MODE>(rp.sw);
+    const int bytes = res_smem_bytes(rp.sw);
     cudaError_t e = cudaFuncSetAttribute(res_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return (int)e;
     void* args[] = {const_cast<ResParams*>(&rp)};
