@@ -456,6 +456,13 @@ def time_config1(engine, torch, dev, stream, peak, with_cpu, mixed=False):
                                             len(items), cells, (fb + bb) * (nt - 1), peak)
     out["gpu_batched_4"] = _config_line("config1", _shot_rate(torch, dev, stream, batched, len(items)), len(items),
                                         cells, (fb + bb) * (nt - 1), peak)
+    engine.set_pass_launch(2)  # each pass one launch, regions resident in shared memory
+    try:
+        out["gpu_resident_one_at_a_time"] = _config_line(
+            "config1", _shot_rate(torch, dev, stream, one_at_a_time, len(items)), len(items), cells,
+            (fb + bb) * (nt - 1), peak, launch="one cooperative launch per pass, regions resident in shared memory")
+    finally:
+        engine.set_pass_launch(0)
     if with_cpu:
         ctx = mp.get_context("spawn")
         t0 = time.perf_counter()

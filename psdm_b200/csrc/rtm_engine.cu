@@ -946,7 +946,7 @@ int build_forward(psdm_engine* e, Shot& s, int nt, int store_snap, const float* 
         CUDA_TRY(cudaMemsetAsync(d_rec, 0, (size_t)nrec * nt * sizeof(float), e->stream));
     }
     StepArgs a = base_args(s);
-    plan_tiles(&a, inj.row_slot.data(), batched);
+    plan_tiles(&a, inj.row_slot.data(), batched, true);
     a.row_slot = d_row;
     a.inj_cols = d_cols;
     a.inj_trace = d_S;

@@ -272,7 +272,8 @@ int launch_pair_batch(const PairBatchParams& bp, int num_sms, void* stream);
 // nx, dn, zoff, fs) and the host copy of the injection row map (ldz
 // entries, or null when nothing is injected).  `batched` plans the interior
 // tiles of batch_step_kernel, otherwise those of step_kernel.
-void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched = false);
+// forward: the plan of a one-shot forward pass (its interior tiles are narrower).
+void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched = false, bool forward = false);
 
 // Set kernel attributes (shared memory carve-out, occupancy); call once per
 // device before the first launch.  Returns a cudaError_t value.

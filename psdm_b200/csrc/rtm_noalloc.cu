@@ -286,7 +286,7 @@ extern "C" int psdm_model_shot_noalloc(const psdm_params* prm, int32_t NumRec, i
     a.err = err;
     for (int i = 0; i < g.ldz; ++i) t_row_slot[i] = -1;
     if (src_interior) t_row_slot[zs + g.zoff] = 0;
-    plan_tiles(&a, t_row_slot);
+    plan_tiles(&a, t_row_slot, false, true);
 
     // k = 2..nt (src/solver_ac_forward_ram.f90:344-577): source sample
     // S(k-1), receivers Rec(k-2) gathered from level k-1.
