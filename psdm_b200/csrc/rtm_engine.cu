@@ -457,7 +457,8 @@ bool pass_form(const std::vector<StepArgs>& args, StepArgs base[2], std::vector<
         if (std::memcmp(&t, &b, sizeof(StepArgs)) != 0) return false;
     }
     const StepArgs &b0 = base[0], &b1 = base[1];
-    return b0.nrect == b1.nrect && b0.itx == b1.itx && std::memcmp(b0.r_type, b1.r_type, sizeof b0.r_type) == 0 &&
+    return b0.nrect == b1.nrect && b0.itx == b1.itx && b0.ixb == b1.ixb &&
+           std::memcmp(b0.r_type, b1.r_type, sizeof b0.r_type) == 0 &&
            std::memcmp(b0.r_zd0, b1.r_zd0, sizeof b0.r_zd0) == 0 && std::memcmp(b0.r_x0, b1.r_x0, sizeof b0.r_x0) == 0 &&
            std::memcmp(b0.r_h, b1.r_h, sizeof b0.r_h) == 0 && std::memcmp(b0.r_w, b1.r_w, sizeof b0.r_w) == 0 &&
            std::memcmp(b0.r_tz, b1.r_tz, sizeof b0.r_tz) == 0 &&
@@ -477,7 +478,7 @@ int launch_pass_form(psdm_engine* e, int mode, const std::vector<StepArgs>& args
     const int nb = pass_blocks_per_sm(mode);
     if (nb <= 0 || ntiles <= 0) return 1;
     const int grid = std::min(ntiles, nb * e->num_sms);
-    std::vector<int> key = {mode == 0 ? a.nrec : 0, a.nrect, a.itx, a.ldz, a.nxt};
+    std::vector<int> key = {mode == 0 ? a.nrec : 0, a.nrect, a.itx, a.ixb, a.ldz, a.nxt};
     key.insert(key.end(), a.r_type, a.r_type + a.nrect);
     key.insert(key.end(), a.r_zd0, a.r_zd0 + a.nrect);
     key.insert(key.end(), a.r_x0, a.r_x0 + a.nrect);

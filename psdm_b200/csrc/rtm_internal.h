@@ -116,6 +116,7 @@ struct StepArgs {
     // [r_first[r], r_first[r+1]) with r_tz tiles along z.
     int nrect;
     int itx;  // interior tile columns the plan was made for (one-shot or batched launches)
+    int ixb;  // C-PML x-strip tile columns the plan was made for (one-shot or batched launches)
     int r_type[16], r_zd0[16], r_x0[16], r_h[16], r_w[16], r_tz[16], r_first[17];
     // persistent scheduling: tile_counter[counter_sel] starts at 0 (cleared
     // by the previous step); num_sms = multiprocessor count of the device

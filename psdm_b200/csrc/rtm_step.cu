@@ -80,6 +80,14 @@ constexpr int PTX = NWARP * PXS;
 constexpr int PHZ = PTZ + 8;
 constexpr int PHQ = PHZ / 4;
 constexpr int PWX = PTX + 6;
+// C-PML x-strip tiles: 128 rows x (4 XXS) columns, each thread 4 rows x XXS
+// columns: 2 columns in one-shot forward passes (the forward step 10.7 ->
+// 10.5 us on config 2, these tiles ending last), 4 otherwise (with 2 the
+// one-shot mixed backward ran 7 %, 8 FP16 shots in flight 3 % and config 4
+// up to 22 % slower).
+constexpr int XXS_ONE = 2, XXS_MANY = PXS;
+template <int MODE, bool BATCHED>
+__host__ __device__ constexpr int xxs() { return (!BATCHED && MODE == 0) ? XXS_ONE : XXS_MANY; }
 // z-strip tiles: 32 rows x 32 columns (8 columns per thread); row-band
 // tiles: 4 rows x 64 columns (2 cells per thread).  Sized so that, with the
 // interior and x-strip tiles, a step has about as many tiles as resident
@@ -369,33 +377,35 @@ __device__ __forceinline__ void rowband_tile(const StepArgs& a, float* ps, int r
 
 // C-PML x-strip over the interior band rows (rect type 1): rows are interior
 // rows (kz = 0, no row clamping), columns x-PML columns.  Each thread owns 4
-// rows (one float4) of 4 columns; the C-PML factor, the clamped stencil
+// rows (one float4) of XXS columns; the C-PML factor, the clamped stencil
 // centre cx and the strip-local phi centre are uniform per column.
-template <int MODE>
-__device__ __forceinline__ void xband_tile(const StepArgs& a, float* ps, int r, int t) {
+template <int MODE, int XXS>
+__device__ __forceinline__ bool xband_tile(const StepArgs& a, float* ps, int r, int t) {
+    constexpr int XTX = NWARP * XXS;  // the plan's a.ixb (checked on the host before a launch)
     const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
-    const int z0 = a.r_zd0[r] + tz * TZ, x0 = a.r_x0[r] + tx * PTX;
+    const int z0 = a.r_zd0[r] + tz * TZ, x0 = a.r_x0[r] + tx * XTX;
     const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
     const int sz0 = z0 - 4;
     const int sx0 = min(x0, a.nxt - 4) - 3;
-    load_tile(a, ps, sz0, sx0, HQ, PWX, tid);
+    load_tile(a, ps, sz0, sx0, HQ, XTX + 6, tid);
     __syncthreads();
     const int zd = z0 + 4 * lane;
-    if (zd >= zend) return;
+    if (zd >= zend) return true;
     const int dn = a.dn;
     const int z = zd - a.zoff;
     const bool fsq = a.fs && z == dn;
     const float4* __restrict__ ps4 = reinterpret_cast<const float4*>(ps);
     const int qr = (zd - sz0) >> 2;
 #pragma unroll 1
-    for (int c = 0; c < PXS; ++c) {
-        const int x = x0 + wy * PXS + c;
+    for (int c = 0; c < XXS; ++c) {
+        const int x = x0 + wy * XXS + c;
         if (x >= xend) break;
         XbandIn in;
         xband_load(a, zd, x, true, in);
         xband_compute<HQ>(a, ps4, nullptr, sx0, qr, zd, fsq, x, in);
     }
+    return true;
 }
 
 // C-PML z-strip over interior columns (rect type 2): kx = 0.  Rows with
@@ -597,7 +607,9 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
             case 0:
                 if (!interior_tile<MODE, xs_one<MODE>()>(a, sm, &bar, phase, r, t)) return;
                 break;
-            case 1: xband_tile<MODE>(a, sm, r, t); break;
+            case 1:
+                if (!xband_tile<MODE, xxs<MODE, false>()>(a, sm, r, t)) return;
+                break;
             case 2: zstrip_tile<MODE, MODE != 2>(a, sm, r, t); break;
             case 4: rowband_tile<MODE>(a, sm, r, t); break;
             default: generic_tile<MODE>(a, sm, r, t); break;
@@ -639,7 +651,7 @@ __device__ __forceinline__ bool run_tile(const StepArgs& a, float* sm, uint64_t*
     const int t = b - a.r_first[r];
     switch (a.r_type[r]) {
         case 0: return interior_tile<MODE, XS, ST, RG>(a, sm, bar, phase, r, t);
-        case 1: xband_tile<MODE>(a, sm, r, t); return true;
+        case 1: return xband_tile<MODE, xxs<MODE, XS == XS_MANY>()>(a, sm, r, t);
         case 2: zstrip_tile<MODE>(a, sm, r, t); return true;
         case 4: rowband_tile<MODE>(a, sm, r, t); return true;
         default: generic_tile<MODE>(a, sm, r, t); return true;
@@ -846,6 +858,7 @@ __global__ void pad_c2_kernel(const float* vp, int ny, int nx, int dn, int nyt, 
 void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched, bool forward) {
     const int TX = tile_cols(batched ? XS_MANY : (forward ? XS_FWD : XS_ONE));
     a->itx = TX;
+    a->ixb = NWARP * ((!batched && forward) ? XXS_ONE : XXS_MANY);
     // Rects of the padded grid (device rows), heaviest first:
     //   type 0  interior band rows without injection / free surface
     //   type 1  x-strip band   rows [d0, d0+ny4) x C-PML columns
@@ -885,7 +898,7 @@ void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched, bool forwar
     auto add = [&](int type, int zd0, int x0, int h, int w) {
         if (h <= 0 || w <= 0) return;
         const int tzsz = (type == 0 || type == 1) ? TZ : (type == 4 ? 4 : PTZ);
-        const int txsz = type == 0 ? TX : (type == 4 ? RTX : (type == 2 ? ZTX : PTX));
+        const int txsz = type == 0 ? TX : (type == 4 ? RTX : (type == 2 ? ZTX : (type == 1 ? a->ixb : PTX)));
         a->r_type[n] = type;
         a->r_zd0[n] = zd0; a->r_x0[n] = x0; a->r_h[n] = h; a->r_w[n] = w;
         a->r_tz[n] = (h + tzsz - 1) / tzsz;
@@ -944,6 +957,7 @@ int batch_blocks_per_sm() {
 
 template <int MODE>
 int launch_mode(const StepArgs& a, cudaStream_t stream) {
+    if (a.ixb != NWARP * xxs<MODE, false>()) return (int)cudaErrorInvalidValue;  // a plan for another launch form
     const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
     const dim3 grid(min(a.r_first[a.nrect], a.num_sms * blocks_per_sm<MODE>()));
     cudaLaunchConfig_t cfg = {};
@@ -1017,7 +1031,7 @@ void tile_rect(const StepArgs& a, int b, int* z0, int* z1, int* x0, int* x1) {
     while (r + 1 < a.nrect && b >= a.r_first[r + 1]) ++r;
     const int t = b - a.r_first[r], type = a.r_type[r];
     const int tzsz = (type == 0 || type == 1) ? TZ : (type == 4 ? 4 : PTZ);
-    const int txsz = type == 0 ? a.itx : (type == 4 ? RTX : (type == 2 ? ZTX : PTX));
+    const int txsz = type == 0 ? a.itx : (type == 4 ? RTX : (type == 2 ? ZTX : (type == 1 ? a.ixb : PTX)));
     const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
     *z0 = a.r_zd0[r] + tz * tzsz;
     *x0 = a.r_x0[r] + tx * txsz;

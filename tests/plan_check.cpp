@@ -3,8 +3,9 @@
 // one-launch-per-pass form (psdm::pass_lists), linked against the built
 // engine library and run on the CPU.
 //
-// Usage: plan_check ny nx dPML fs batched nrec [injection rows (0-based interior rows)...]
-// Prints: ntiles itx cover_errors dead_errors type_errors sym_errors rec_errors
+// Usage: plan_check ny nx dPML fs form nrec [injection rows (0-based interior rows)...]
+//   form: 0 one-shot backward pass, 1 batched launch, 2 one-shot forward pass
+// Prints: ntiles itx ixb cover_errors dead_errors type_errors sym_errors rec_errors
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -17,7 +18,8 @@ using namespace psdm;
 int main(int argc, char** argv) {
     if (argc < 7) return 2;
     const int ny = atoi(argv[1]), nx = atoi(argv[2]), dPML = atoi(argv[3]), fs = atoi(argv[4]);
-    const bool batched = atoi(argv[5]) != 0;
+    const int form = atoi(argv[5]);
+    const bool batched = form == 1;
     const int nrec = atoi(argv[6]);
     StepArgs a;
     std::memset(&a, 0, sizeof a);
@@ -31,7 +33,7 @@ int main(int argc, char** argv) {
     a.fs = fs;
     std::vector<int> row_slot(a.ldz, -1);
     for (int k = 7; k < argc; ++k) row_slot[a.zoff + a.dn + atoi(argv[k])] = 0;
-    plan_tiles(&a, row_slot.data(), batched);
+    plan_tiles(&a, row_slot.data(), batched, form == 2);
     const int n = a.r_first[a.nrect];
     // every live cell of the padded grid in exactly one tile; the rows above
     // a free surface in none
@@ -107,6 +109,6 @@ int main(int argc, char** argv) {
         }
     for (int i = 0; i < nrec; ++i)
         if (seen[i] != 1) ++rec_err;
-    printf("%d %d %ld %ld %ld %ld %ld\n", n, a.itx, cover_err, dead_err, type_err, sym_err, rec_err);
+    printf("%d %d %d %ld %ld %ld %ld %ld\n", n, a.itx, a.ixb, cover_err, dead_err, type_err, sym_err, rec_err);
     return 0;
 }

@@ -1,7 +1,7 @@
 """The tile planner on the CPU: psdm::plan_tiles / tile_rect cover every live
 cell of the padded grid exactly once (and no cell above a free surface),
 keep injection and free-surface rows out of the interior tiles, use the
-interior tile width of the launch form, and psdm::pass_lists gives
+interior and x-strip tile widths of the launch form and pass, and psdm::pass_lists gives
 symmetric neighbour lists that hold every tile within the read halo and puts
 each receiver in the tile that owns its cell.  tests/plan_check.cpp is
 compiled against the built engine library and run here, without a GPU."""
@@ -29,8 +29,8 @@ def checker(engine_lib, tmp_path_factory):
     return out
 
 
-def _run(checker, ny, nx, dPML, fs, batched, nrec, rows=()):
-    r = subprocess.run([checker, str(ny), str(nx), str(dPML), str(fs), str(int(batched)), str(nrec),
+def _run(checker, ny, nx, dPML, fs, form, nrec, rows=()):
+    r = subprocess.run([checker, str(ny), str(nx), str(dPML), str(fs), str(int(form)), str(nrec),
                         *map(str, rows)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     return [int(v) for v in r.stdout.split()]
@@ -44,16 +44,18 @@ def _run(checker, ny, nx, dPML, fs, batched, nrec, rows=()):
     (1200, 1136, 50, 1, (0, 1), 480),    # config-2 window
     (1800, 1361, 50, 1, (0, 1, 2, 3, 40), 120),
 ])
-@pytest.mark.parametrize("batched", [False, True])
-def test_plan_covers_grid_once(checker, ny, nx, dPML, fs, rows, nrec, batched):
-    n, itx, cover, dead, typ, sym, rec = _run(checker, ny, nx, dPML, fs, batched, nrec, rows)
+@pytest.mark.parametrize("form", [0, 1, 2])  # one-shot backward, batched, one-shot forward
+def test_plan_covers_grid_once(checker, ny, nx, dPML, fs, rows, nrec, form):
+    n, itx, ixb, cover, dead, typ, sym, rec = _run(checker, ny, nx, dPML, fs, form, nrec, rows)
     assert n > 0
-    assert itx == (32 if batched else 28)
+    assert itx == {0: 28, 1: 32, 2: 24}[form]
+    assert ixb == (8 if form == 2 else 16)
     assert (cover, dead, typ, sym, rec) == (0, 0, 0, 0, 0)
 
 
-def test_config2_plan_fits_one_wave(checker):
-    """The config-2 one-shot plan has fewer tiles than the 5 x 148 resident
-    blocks of a step launch."""
-    n, *_ = _run(checker, 1200, 1136, 50, 1, False, 0, (0, 1))
+@pytest.mark.parametrize("form", [0, 2])
+def test_config2_plan_fits_one_wave(checker, form):
+    """The config-2 one-shot plans (backward and forward) have no more tiles
+    than the 5 x 148 resident blocks of a step launch."""
+    n, *_ = _run(checker, 1200, 1136, 50, 1, form, 0, (0, 1))
     assert 500 < n <= 740
