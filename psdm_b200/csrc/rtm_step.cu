@@ -525,6 +525,113 @@ __device__ __forceinline__ void zstrip_tile(const StepArgs& a, float* ps, int r,
     }
 }
 
+// The z-strip tile with every global input of its C-PML cells staged in
+// shared memory before the update (one-shot FP32 launches): phi_z over the
+// p tile's 40-row window (the strip-local stencils of the tile's rows lie in
+// it, as the clamped p stencils do), chi_z, level n-1 and c2 over the tile's
+// 32 rows, all issued as 16-byte cp.async copies together with the p tile's
+// loads, so that a thread's columns wait for one round trip instead of one
+// per column.  The arithmetic is zstrip_tile's, in its order.
+#ifndef PSDM_ZSTRIP_STAGE
+#define PSDM_ZSTRIP_STAGE 1
+#endif
+constexpr bool kZstripStage = PSDM_ZSTRIP_STAGE != 0;
+constexpr int kZsFloats = ZWX * PHZ + ZTX * PHZ + 3 * ZTX * PTZ;
+template <int MODE>
+__device__ __forceinline__ void zstrip_tile_staged(const StepArgs& a, float* ps, int r, int t) {
+    const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
+    const int tz = t % a.r_tz[r], tx = t / a.r_tz[r];
+    const int z0 = a.r_zd0[r] + tz * PTZ, x0 = a.r_x0[r] + tx * ZTX;
+    const int zend = a.r_zd0[r] + a.r_h[r], xend = a.r_x0[r] + a.r_w[r];
+    const int nr = a.zoff + a.nyt;
+    const int sz0 = (min(z0, nr - 4) - 3) & ~3;
+    const int sx0 = x0 - 3;  // interior columns: no clamping along x
+    float* fs = ps + ZWX * PHZ;   // phi_z, ZTX columns of PHZ rows from sz0
+    float* cs = fs + ZTX * PHZ;   // chi_z, ZTX columns of PTZ rows from z0
+    float* ms = cs + ZTX * PTZ;   // level n-1
+    float* c2s = ms + ZTX * PTZ;  // c2
+    // phi_z window (PHZ / 4 float4 per column) and the three tile arrays
+    // (PTZ / 4 each); z0 and sz0 are multiples of 4
+    constexpr int kF4 = PHZ / 4, kT4 = PTZ / 4;
+    for (int q = tid; q < ZTX * (kF4 + 3 * kT4); q += NT) {
+        int col, arr, r4;
+        if (q < ZTX * kF4) {
+            col = q / kF4;
+            r4 = q - col * kF4;
+            arr = 0;
+        } else {
+            const int u = q - ZTX * kF4;
+            arr = 1 + u / (ZTX * kT4);
+            const int v = u - (arr - 1) * ZTX * kT4;
+            col = v / kT4;
+            r4 = v - col * kT4;
+        }
+        const int x = x0 + col;
+        const int row = (arr == 0 ? sz0 : z0) + 4 * r4;
+        if (x >= xend || row < 0 || row + 4 > a.ldz) continue;
+        const size_t gsrc = (size_t)x * a.ldz + row;
+        if (arr == 0) cp_async16(fs + col * PHZ + 4 * r4, a.phiz_in + gsrc);
+        else if (arr == 1) cp_async16(cs + col * PTZ + 4 * r4, a.chiz + gsrc);
+        else if (arr == 2) cp_async16(ms + col * PTZ + 4 * r4, a.pm + gsrc);
+        else cp_async16(c2s + col * PTZ + 4 * r4, a.c2 + gsrc);
+    }
+    cp_async_commit();
+    load_tile(a, ps, sz0, sx0, PHQ, ZWX, tid);
+    cp_async_wait_all();
+    __syncthreads();
+    const int zd = z0 + lane;
+    if (zd >= zend) return;
+    const int dn = a.dn;
+    const int z = zd - a.zoff;
+    if (z < 0 || z >= a.nyt) return;
+    const int kz = (z < dn) ? (dn - z) : (z >= dn + a.ny ? z - (dn + a.ny) + 1 : 0);
+    if (kz == 0) {
+#pragma unroll 1
+        for (int c = 0; c < ZXS; ++c) {
+            const int x = x0 + wy * ZXS + c;
+            if (x >= xend) break;
+            cell_generic<MODE, PHZ>(a, ps, sz0, sx0, zd, x);
+        }
+        return;
+    }
+    const float A = __ldg(a.fA + kz - 1), B = __ldg(a.fB + kz - 1);
+    const int zl = zd - sz0;
+    const int czl = clampi(z, 3, a.nyt - 4) + a.zoff - sz0;
+    const int sb = (z < dn) ? 0 : dn + a.ny;
+    const int cjl = clampi(z - sb, 3, dn - 4) + sb + a.zoff - sz0;  // phi_z stencil centre in the window
+    const int tl = zd - z0;                                          // row in the tile arrays
+    const float* c1 = a.cf1;
+    const float* c2 = a.cf2;
+#pragma unroll 1
+    for (int c = 0; c < ZXS; ++c) {
+        const int cl = wy * ZXS + c;  // tile column
+        const int x = x0 + cl;
+        if (x >= xend) break;
+        const int xl = x - sx0;
+        const float* colc = ps + xl * PHZ + zl;
+        const float* colz = ps + xl * PHZ + czl;
+        const float* phs = fs + cl * PHZ;
+#define AX(k) colc[(k) * PHZ]
+#define AZ(k) colz[(k)]
+#define PZ(k) phs[cjl + (k)]
+        const float d2x = D2(AX, c2);
+        const float d2y = D2(AZ, c2);
+        const float d1 = D1(AZ, c1);
+        const float dph = D1(PZ, c1);
+#undef AX
+#undef AZ
+#undef PZ
+        const int g = x * a.ldz + zd;
+        const float phn = __fadd_rn(__fmul_rn(A, phs[zl]), __fmul_rn(B, d1));
+        const float chn = __fadd_rn(__fmul_rn(A, cs[cl * PTZ + tl]), __fmul_rn(B, __fadd_rn(d2y, dph)));
+        a.phiz_out[g] = phn;
+        a.chiz[g] = chn;
+        const float prop = __fadd_rn(dph, chn);
+        const float base = __fadd_rn(-ms[cl * PTZ + tl], __fmul_rn(2.f, colc[0]));
+        a.pm[g] = __fadd_rn(base, __fmul_rn(c2s[cl * PTZ + tl], __fadd_rn(__fadd_rn(d2x, d2y), prop)));
+    }
+}
+
 // Corner tiles and anything else (rect type 3): generic per-cell update.
 template <int MODE>
 __device__ __forceinline__ void generic_tile(const StepArgs& a, float* ps, int r, int t) {
@@ -610,7 +717,10 @@ __global__ void __launch_bounds__(NT, 5) step_kernel(const StepArgs a) {
             case 1:
                 if (!xband_tile<MODE, xxs<MODE, false>()>(a, sm, r, t)) return;
                 break;
-            case 2: zstrip_tile<MODE, MODE != 2>(a, sm, r, t); break;
+            case 2:
+                if (kZstripStage && MODE != 2) zstrip_tile_staged<MODE>(a, sm, r, t);
+                else zstrip_tile<MODE, MODE != 2>(a, sm, r, t);
+                break;
             case 4: rowband_tile<MODE>(a, sm, r, t); break;
             default: generic_tile<MODE>(a, sm, r, t); break;
         }
@@ -929,11 +1039,15 @@ void plan_tiles(StepArgs* a, const int* row_slot_host, bool batched, bool forwar
     a->nrect = n;
 }
 
+// Dynamic shared memory of the one-shot step kernel: an interior tile's p
+// tile, or a staged z-strip tile.
+constexpr int step_smem_floats() { return smem_floats<XS_ONE>() > kZsFloats ? smem_floats<XS_ONE>() : kZsFloats; }
+
 template <int MODE>
 int blocks_per_sm() {
     static int nb = 0;
     if (nb == 0) {
-        const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
+        const int bytes = step_smem_floats() * (int)sizeof(float);
         cudaFuncSetAttribute(step_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<MODE>, NT, bytes);
@@ -958,7 +1072,7 @@ int batch_blocks_per_sm() {
 template <int MODE>
 int launch_mode(const StepArgs& a, cudaStream_t stream) {
     if (a.ixb != NWARP * xxs<MODE, false>()) return (int)cudaErrorInvalidValue;  // a plan for another launch form
-    const int bytes = smem_floats<XS_ONE>() * (int)sizeof(float);
+    const int bytes = step_smem_floats() * (int)sizeof(float);
     const dim3 grid(min(a.r_first[a.nrect], a.num_sms * blocks_per_sm<MODE>()));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
