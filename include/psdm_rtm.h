@@ -298,6 +298,17 @@ int32_t psdm_engine_batch_slots(const psdm_engine* e);
 int psdm_engine_check_wait_timeout(psdm_engine* e);
 
 /*
+ * The snapshot quotient of the forward kernels, x / dt, for n host inputs (no
+ * counterpart: the reference divides in FP32 when it stores a snapshot,
+ * src/solver_ac_forward_ram.f90:485): q[i] as the interior tiles compute it (a branch-free
+ * form, with the general one for a float4 holding a rare input), q[n + i] by
+ * the general form alone.  Both must equal the IEEE quotient x / dt rounded
+ * to nearest, subnormal results and signed zeros included.  n is a positive
+ * multiple of 4; q holds 2 n floats.
+ */
+int psdm_engine_dt_quotients(psdm_engine* e, float dt, const float* x, int32_t n, float* q);
+
+/*
  * Forward modelling only (the receiver output Rec_point of
  * solver_ac_forward_ram, src/solver_ac_forward_ram.f90:567-577) without
  * storing snapshots: synthetic shot gathers for least-squares or QC.

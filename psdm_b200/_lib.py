@@ -23,7 +23,7 @@ EXPORTS = [
     "psdm_rtm_shot", "psdm_rtm_shot_device", "psdm_model_shot", "psdm_fd_coef", "psdm_pml_coeffs", "psdm_ricker_mcs",
     "psdm_dynamic_window", "psdm_taper_pad_trace", "psdm_optimization_dt", "psdm_normalize_psdm",
     "psdm_model_shot_noalloc", "psdm_plan_memory", "psdm_engine_autotune", "psdm_rtm_shot_fp64", "psdm_rtm_batch", "psdm_rtm_batch_device", "psdm_engine_batch_slots",
-    "psdm_engine_check_wait_timeout", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
+    "psdm_engine_check_wait_timeout", "psdm_engine_dt_quotients", "psdm_trace_windows", "psdm_condition_traces", "psdm_condition_traces_device",
     "psdm_su_write_image", "psdm_su_read_shot", "psdm_su_read_header_i32", "psdm_engine_set_checkpointing", "psdm_engine_set_pass_launch", "psdm_engine_set_steps_per_launch", "psdm_engine_set_reconstruction",
     "psdm_freq_filter", "psdm_freq_filter_device", "psdm_butterworth_response",
     "psdm_nav_read", "psdm_channel_positions", "psdm_geometry_mcs", "psdm_linear_2d", "psdm_batmodel_from_velocity",
@@ -114,6 +114,7 @@ def lib():
     L.psdm_engine_batch_slots.argtypes = [_P]
     L.psdm_engine_batch_slots.restype = _I
     L.psdm_engine_check_wait_timeout.argtypes = [_P]
+    L.psdm_engine_dt_quotients.argtypes = [_P, _F, _f32p, _I, _f32p]
     L.psdm_engine_set_checkpointing.argtypes = [_P, _I]
     L.psdm_engine_set_pass_launch.argtypes = [_P, _I]
     L.psdm_engine_set_steps_per_launch.argtypes = [_P, _I]

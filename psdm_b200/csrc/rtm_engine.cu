@@ -2680,6 +2680,27 @@ int psdm_engine_check_wait_timeout(psdm_engine* e) {
     return sync(e);
 }
 
+int psdm_engine_dt_quotients(psdm_engine* e, float dt, const float* x, int32_t n, float* q) {
+    TRY(check_engine(e));
+    if (!x || !q || n <= 0 || n % 4) return fail(PSDM_ERR_ARG, "null argument, or n not a positive multiple of 4");
+    TRY(sync(e));
+    auto it = e->div_cache.find(dt);
+    if (it == e->div_cache.end()) {
+        float r = 0.f, lo = 0.f, hi = 0.f, tiny = 0.f;
+        const int ok = fast_div_exact(dt, &r, &lo, &hi, &tiny) ? 1 : 0;
+        it = e->div_cache.emplace(dt, std::make_pair(ok, std::vector<float>{r, lo, hi, tiny})).first;
+    }
+    const std::vector<float>& c = it->second.second;
+    float *d_x = nullptr, *d_q = nullptr;
+    TRY(e->get("dq_x", (size_t)n, &d_x));
+    TRY(e->get("dq_q", (size_t)2 * n, &d_q));
+    CUDA_TRY(cudaMemcpyAsync(d_x, x, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    const int rc = launch_dt_quotients(dt, c[0], c[1], c[2], it->second.first, d_x, d_q, n, e->stream);
+    if (rc) return fail(PSDM_ERR_CUDA, "quotient launch: %s", cudaGetErrorString((cudaError_t)rc));
+    CUDA_TRY(cudaMemcpyAsync(q, d_q, (size_t)2 * n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    return sync(e);
+}
+
 int psdm_model_shot(psdm_engine* e, const psdm_params* prm, int32_t NumRec, int32_t nxSou, int32_t nySou,
                     const int32_t* nxRec, const int32_t* nyRec, const float* Data_source, float dd, float dt,
                     int32_t ny, int32_t nx, int32_t nx_w, const float* Vp_w, float dd_space, int32_t nt,

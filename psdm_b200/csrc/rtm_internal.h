@@ -415,6 +415,8 @@ int launch_resident(int mode, const ResParams& rp, void* stream);
 
 // One kernel whose bounded copy wait runs out (nothing is copied); sets *err.
 int launch_wait_timeout_probe(int* err, void* stream);
+int launch_dt_quotients(float dt, float inv_dt, float div_lo, float div_hi, int fast_div, const float* x, float* q,
+                        int n, void* stream);
 // Launch one batched step (batch_step_kernel) on `stream`.
 int launch_batch_step(const BatchParams& bp, int num_sms, void* stream);
 // Receiver gather after the last forward step (Rec(nt-1) and Rec(nt)).

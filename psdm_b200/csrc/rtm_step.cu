@@ -1257,6 +1257,37 @@ int launch_wait_timeout_probe(int* err, void* stream) {
     return (int)cudaGetLastError();
 }
 
+// The snapshot quotient x / dt of the forward kernels for n inputs: q[i] by
+// the interior tiles' form (div_dt_common for a float4, div_dt for all four
+// when any of them is rare), q[n + i] by div_dt alone.  n is a multiple of 4.
+__global__ void dt_quotients_kernel(const StepArgs a, const float* x, float* q, int n) {
+    const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const float4 v = *reinterpret_cast<const float4*>(x + i);
+    bool rare = false;
+    float4 sv;
+    sv.x = div_dt_common(a, v.x, rare);
+    sv.y = div_dt_common(a, v.y, rare);
+    sv.z = div_dt_common(a, v.z, rare);
+    sv.w = div_dt_common(a, v.w, rare);
+    if (rare) sv = make_float4(div_dt(a, v.x), div_dt(a, v.y), div_dt(a, v.z), div_dt(a, v.w));
+    *reinterpret_cast<float4*>(q + i) = sv;
+    *reinterpret_cast<float4*>(q + n + i) = make_float4(div_dt(a, v.x), div_dt(a, v.y), div_dt(a, v.z), div_dt(a, v.w));
+}
+
+int launch_dt_quotients(float dt, float inv_dt, float div_lo, float div_hi, int fast_div, const float* x, float* q,
+                        int n, void* stream) {
+    if (n <= 0 || n % 4) return (int)cudaErrorInvalidValue;
+    StepArgs a{};
+    a.dt = dt;
+    a.inv_dt = inv_dt;
+    a.div_lo = div_lo;
+    a.div_hi = div_hi;
+    a.fast_div = fast_div;
+    dt_quotients_kernel<<<(n / 4 + 127) / 128, 128, 0, (cudaStream_t)stream>>>(a, x, q, n);
+    return (int)cudaGetLastError();
+}
+
 int launch_rec_final(const int* rec_cell, const float* p, float* rec_out, int nrec, int rec_ld, int nt, void* stream) {
     if (nrec <= 0 || nt < 2) return 0;
     rec_final_kernel<<<(nrec + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rec_cell, p, rec_out, nrec, rec_ld, nt);

@@ -248,6 +248,13 @@ class Engine:
         """psdm_engine_check_wait_timeout: raises PsdmError when the failure path works."""
         L.check(L.lib().psdm_engine_check_wait_timeout(self._h))
 
+    def dt_quotients(self, dt: float, x):
+        """psdm_engine_dt_quotients: (the interior tiles' x / dt, the general form's x / dt), float32."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        q = np.zeros(2 * x.size, dtype=np.float32)
+        L.check(L.lib().psdm_engine_dt_quotients(self._h, float(dt), x, int(x.size), q))
+        return q[:x.size], q[x.size:]
+
     def batch_slots(self) -> int:
         return int(L.lib().psdm_engine_batch_slots(self._h))
 
